@@ -1,0 +1,235 @@
+/*
+ * lbm_b200.h — C ABI of the B200 lattice-Boltzmann time-step library.
+ *
+ * This is the drop-in boundary for the time-step hot path of LBMengine.jl
+ * (GPU module).  The reference has no FFI layer of its own: its boundary is
+ * the exported Julia API (src/LBMengine.jl:27-41) and the fields of
+ * `LBMmodel` / `LBMparticle` (src/gpu/structs.jl:52-95).  Each entry point
+ * below names the reference function whose effect it reproduces; a Julia
+ * shim binds them with `ccall`, a Python mirror binds
+ * them with ctypes (lbmengine.jl_b200/lbmengine/_capi.py).
+ *
+ * Conventions
+ *   - Every function returns an int status: 0 = LBM_OK, < 0 = error.  The
+ *     message of the last failure is returned by lbm_last_error(h) (or by
+ *     lbm_last_global_error() when no handle exists yet).
+ *   - All caller buffers are HOST memory owned by the caller, FP64, in the
+ *     reference's column-major order: scalar fields (N...) with x fastest,
+ *     vector fields (N..., d) and populations (N..., Q) with the component /
+ *     direction index slowest.  Cell index = x + nx*(y + ny*z).
+ *   - The library owns all device memory; a handle is not thread-safe and
+ *     issues all its work on one CUDA stream.
+ *   - Lattice units follow the reference's GPU module: the time step equals
+ *     the lattice parameter (dt == dx, src/gpu/initMethods.jl:475-492) and the
+ *     lattice speed is 1.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBM_OK               0
+#define LBM_ERR_INVALID     -1  /* bad argument (mirrors the reference's @assert / error sites) */
+#define LBM_ERR_CUDA        -2  /* CUDA runtime failure */
+#define LBM_ERR_OOM         -3  /* device allocation failed */
+#define LBM_ERR_UNSUPPORTED -4  /* valid in the reference, not supported by this build */
+#define LBM_ERR_NUMERIC     -5  /* NaN/Inf or non-positive density detected on device */
+#define LBM_ERR_TIMEOUT     -6  /* a bounded device wait gave up */
+#define LBM_ERR_STATE       -7  /* call not valid in the handle's current state */
+#define LBM_ERR_NO_DEVICE   -8  /* no CUDA device / extension not usable */
+
+/* ---- enumerations ------------------------------------------------------ */
+/* velocity sets, src/gpu/misc.jl:195-272 */
+#define LBM_D2Q9   9
+#define LBM_D3Q15 15
+#define LBM_D3Q19 19
+#define LBM_D3Q27 27
+
+/* collision model, src/gpu/fluids.jl:58-101 */
+#define LBM_BGK 0
+#define LBM_TRT 1
+
+/* population storage on the device (the reference stores FP64 everywhere) */
+#define LBM_STORE_F32  0   /* shifted FP32: (f_i/w_i - rho0) */
+#define LBM_STORE_F16  1   /* shifted FP16: (f_i/w_i - rho0) * store_scale */
+#define LBM_STORE_BF16 2   /* shifted BF16: (f_i/w_i - rho0) * store_scale */
+#define LBM_STORE_F64  3   /* shifted FP64 (high-precision reference runs) */
+
+/* particle kinds, src/gpu/initMethods.jl:7 (addBead!) and :91 (addSquirmer!) */
+#define LBM_BEAD     0
+#define LBM_SQUIRMER 1
+
+/* force modes, src/gpu/initMethods.jl:636-654 */
+#define LBM_FORCE_NONE    0
+#define LBM_FORCE_UNIFORM 1   /* constant vector, zeroed on wall nodes */
+#define LBM_FORCE_FIELD   2   /* (N..., d) field, zeroed on wall nodes */
+
+/* ---- model configuration: the resolved keyword set of modelInit ---------
+ * Replaces modelInit(; ...) src/gpu/initMethods.jl:440-702.  Keyword
+ * resolution (tau from viscosity, default limits, walls from a Julia
+ * function, ...) is done by the host shim; this struct carries the result. */
+typedef struct lbm_config {
+    int32_t dims;              /* 2 or 3 */
+    int32_t lattice;           /* LBM_D2Q9 / LBM_D3Q15 / LBM_D3Q19 / LBM_D3Q27 */
+    int64_t n[3];              /* nodes per axis; n[2] == 1 when dims == 2 */
+    const double* coords[3];   /* node coordinates per axis (length n[a]), or NULL */
+    double x0[3];              /* used when coords[a] == NULL: x = x0[a] + i*dx */
+    double dx;                 /* lattice parameter == time step */
+    double tau;                /* relaxation time (relaxationTimeRatio * dt); tau+ for TRT */
+    double tau_minus;          /* TRT tau- (kineticParameter*c_s^2*dt^2/nu + dt/2), ignored for BGK */
+    int32_t collision;         /* LBM_BGK / LBM_TRT */
+    int32_t compressible;      /* isFluidCompressible (src/gpu/fluids.jl:50-51) */
+    int32_t force_mode;        /* LBM_FORCE_* */
+    int32_t storage;           /* LBM_STORE_* */
+    double force[3];           /* uniform force density (force_mode == LBM_FORCE_UNIFORM) */
+    const double* force_field; /* (N..., d) (force_mode == LBM_FORCE_FIELD) */
+    const uint8_t* wall_mask;  /* (N...) solid wall nodes, or NULL (no bounce-back walls) */
+    const double* wall_velocity; /* (N..., d) moving-wall velocity, or NULL */
+    const double* rho_init;    /* (N...) initial density, or NULL -> rho_uniform */
+    const double* u_init;      /* (N..., d) initial velocity, or NULL -> u_uniform */
+    double rho_uniform;        /* initial density when rho_init == NULL */
+    double u_uniform[3];       /* initial velocity when u_init == NULL */
+    double rho_ref;            /* shift density rho0 of the stored populations (0 -> 1.0) */
+    double store_scale;        /* power-of-two scale for F16/BF16 storage (0 -> default 2^12) */
+    int32_t device;            /* CUDA device ordinal; < 0: the calling thread's current device */
+    int32_t reserved0;
+} lbm_config;
+
+/* ---- particle parameters: the resolved keyword set of addBead!/addSquirmer!
+ * Replaces src/gpu/initMethods.jl:7-89 and :91-222.  The shim resolves B1/B2
+ * from swimmingSpeed/slipSpeed/beta and normalises and signs the swimming
+ * direction (:133-173); the library computes the mass exactly as the
+ * reference does (node count of an origin-centred sphere, :108) and the
+ * moment of inertia (:117-127). */
+typedef struct lbm_particle_params {
+    int32_t kind;              /* LBM_BEAD / LBM_SQUIRMER */
+    int32_t couple_forces;     /* coupleForces */
+    int32_t couple_torques;    /* coupleTorques */
+    int32_t reserved;
+    double radius;
+    double mass_density;
+    double position[3];
+    double velocity[3];
+    double angular_velocity[3];   /* 2D: angular_velocity[0] is the scalar omega */
+    double swimming_direction[3]; /* squirmer only; already normalised and signed */
+    double B1, B2;                /* squirmer only */
+} lbm_particle_params;
+
+/* ---- particle state (read back) ----------------------------------------
+ * Mirrors LBMparticle (src/gpu/structs.jl:85-95) after a tick. */
+typedef struct lbm_particle_state {
+    int32_t id;                /* 1-based, as LBMparticle.id */
+    int32_t kind;
+    int32_t couple_forces;
+    int32_t couple_torques;
+    double radius;
+    double inverse_mass;
+    double inverse_inertia;
+    double B1, B2;
+    double position[3];
+    double velocity[3];
+    double angular_velocity[3];   /* 2D: [0] */
+    double swimming_direction[3];
+    double last_force[3];      /* momentum-exchange force of the last tick (forceInput before reset) */
+    double last_torque[3];     /* 2D: [0] */
+} lbm_particle_state;
+
+typedef struct lbm_info {
+    int32_t dims, lattice, q, storage;
+    int64_t n[3];
+    int64_t cells;
+    int64_t tick;
+    double time;
+    int32_t num_particles;
+    int32_t bytes_per_population;  /* storage bytes of one population value */
+    int64_t device_bytes;          /* device memory held by the handle */
+} lbm_info;
+
+typedef struct lbm_handle lbm_handle;
+
+/* Library identity. */
+int32_t lbm_abi_version(void);
+const char* lbm_build_info(void);
+
+/* modelInit(; ...)  src/gpu/initMethods.jl:440-702 (with findInitialConditions
+ * :417-438 and the initial hydroVariablesUpdate! src/gpu/fluids.jl:32). */
+int lbm_create(const lbm_config* cfg, lbm_handle** out);
+
+/* addBead! / addSquirmer!  src/gpu/initMethods.jl:7-89 / :91-222, including
+ * the initial-setup moveParticles! (src/gpu/particles.jl:7-92).
+ * *id_out receives the 1-based particle id. */
+int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_out);
+
+/* LBMpropagate!(model; ticks = nsteps)  src/gpu/fluids.jl:228-264: nsteps
+ * calls of tick! (:132-226), each = collision + streaming + bounce-back +
+ * moving walls + Ladd coupling + hydro update + particle update. */
+int lbm_step(lbm_handle* h, int64_t nsteps);
+
+/* model.massDensity (N...) and model.fluidVelocity (N..., d) after the last
+ * tick (hydroVariablesUpdate!, src/gpu/fluids.jl:32-37).  Either may be NULL. */
+int lbm_get_fields(lbm_handle* h, double* rho, double* u);
+
+/* model.distributions (N..., Q), FP64. */
+int lbm_get_distributions(lbm_handle* h, double* f);
+
+/* Overwrite the populations (N..., Q) from the host (checkpoint restore). */
+int lbm_set_distributions(lbm_handle* h, const double* f);
+
+/* model.particles[...] state; writes min(capacity, P) entries, *count = P. */
+int lbm_get_particles(lbm_handle* h, lbm_particle_state* out, int32_t capacity, int32_t* count);
+
+/* Overwrite position / velocity / angular velocity / swimming direction of
+ * particle `id` (1-based) and re-voxelise it (moveParticles! initialSetup). */
+int lbm_set_particle(lbm_handle* h, int32_t id, const lbm_particle_state* s);
+
+/* particle.boundaryConditionsParams.solidRegion (N...) as 0/1 bytes
+ * (getSphere, src/gpu/aux.jl:206-215), for particle `id` (1-based). */
+int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask);
+
+/* Boundary links of particle `id`: the (cell, direction) pairs of
+ * streamingInvasionRegions (bounceBackPrep, src/gpu/aux.jl:187-198), i.e.
+ * fluid cells x with x - c_dir solid, as 0-based cell index and 0-based
+ * direction index, sorted by (direction, cell).  With cells == NULL only the
+ * count is returned in *n. */
+int lbm_get_links(lbm_handle* h, int32_t id, int64_t* cells, int8_t* dirs, int64_t capacity, int64_t* n);
+
+int lbm_get_info(lbm_handle* h, lbm_info* info);
+
+/* Device-time profile of the most recent lbm_step call (CUDA events on the
+ * handle's stream; with profiling on, event nodes are captured around every
+ * kernel of the step graph).  No counterpart in the reference, which has no
+ * tracing (only a `verbose` progress print, src/gpu/fluids.jl:229-253). */
+typedef struct lbm_profile {
+    double total_ms;        /* device time of the whole lbm_step call */
+    double bulk_ms;         /* mean duration of one bulk stream-collide launch */
+    double boundary_ms;     /* mean duration of one boundary-tile launch (0 if none) */
+    double particles_ms;    /* mean duration of one particle-update launch (0 if none) */
+    int64_t steps;          /* ticks in the call */
+    int64_t launches;       /* kernel launches enqueued by the call */
+    int64_t profiled_steps; /* ticks whose kernels were bracketed by events */
+    int64_t bulk_cells;     /* lattice nodes updated by the bulk kernel in the last tick */
+    int64_t boundary_tiles; /* tiles handled by the boundary kernel in the last tick */
+} lbm_profile;
+
+int lbm_set_profiling(lbm_handle* h, int32_t on);
+int lbm_get_profile(lbm_handle* h, lbm_profile* out);
+
+/* Raw checkpoint of populations + particle FP64 state + tick/time. */
+int lbm_save_state(lbm_handle* h, const char* path);
+int lbm_load_state(lbm_handle* h, const char* path);
+
+const char* lbm_last_error(lbm_handle* h);
+const char* lbm_last_global_error(void);
+void lbm_destroy(lbm_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

@@ -1,0 +1,184 @@
+// Set-up and read-back kernels (not on the per-tick path).
+#pragma once
+#include "kernels.cuh"
+
+namespace lbm {
+
+struct CodecArgs {
+    void* pop;            // stored populations
+    double* f64;          // [Q][N] FP64 populations (f units)
+    double* rho;          // [N] or null
+    double* u;            // [d][N] or null
+    const unsigned char* wall;
+    const double* ffield;
+    long long N;
+    double rho0, scale, inv_scale, half_dt;
+    double F[3];
+    int force_mode;
+};
+
+// f (FP64, reference units) -> stored g = (f/w - rho0)*scale
+template <class L, int ST>
+__global__ void k_encode(const CodecArgs a) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    using R = typename SS::R;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    T* pop = static_cast<T*>(a.pop);
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const double g = a.f64[i * a.N + c] * (1.0 / L::w(i)) - a.rho0;
+        pop[i * a.N + c] = SS::enc((R)g, (R)a.scale);
+    }
+}
+
+// stored g -> f (FP64); wall nodes hold f = 0 exactly
+template <class L, int ST>
+__global__ void k_decode(const CodecArgs a) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    const T* pop = static_cast<const T*>(a.pop);
+    const bool w = a.wall && a.wall[c];
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const double g = (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale);
+        a.f64[i * a.N + c] = w ? 0.0 : L::w(i) * (a.rho0 + g);
+    }
+}
+
+// hydroVariablesUpdate! (src/gpu/fluids.jl:7-37) from the stored populations, in FP64
+template <class L, int ST>
+__global__ void k_macro(const CodecArgs a) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    const T* pop = static_cast<const T*>(a.pop);
+    if (a.wall && a.wall[c]) {
+        if (a.rho) a.rho[c] = 0.0;
+        if (a.u)
+            for (int k = 0; k < L::D; ++k) a.u[k * a.N + c] = 0.0;
+        return;
+    }
+    double drho = 0, j[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const double wg = L::w(i) * (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale);
+        drho += wg;
+        j[0] += L::cx(i) * wg;
+        j[1] += L::cy(i) * wg;
+        j[2] += L::cz(i) * wg;
+    }
+    const double rho = a.rho0 + drho;
+    double F[3] = {0, 0, 0};
+    if (a.force_mode == 1) {
+        F[0] = a.F[0];
+        F[1] = a.F[1];
+        F[2] = a.F[2];
+    } else if (a.force_mode == 2) {
+        for (int k = 0; k < L::D; ++k) F[k] = a.ffield[k * a.N + c];
+    }
+    if (a.rho) a.rho[c] = rho;
+    if (a.u)
+        for (int k = 0; k < L::D; ++k) a.u[k * a.N + c] = rho == 0.0 ? 0.0 : (j[k] + a.half_dt * F[k]) / rho;
+}
+
+
+struct InitArgs {
+    void* pop;
+    long long N;
+    const double* rho;      // [N] or null -> rho_uniform
+    const double* u;        // [d][N] or null -> u_uniform
+    const unsigned char* wall;
+    const double* ffield;   // [d][N] (already zero on walls) or null
+    double rho_uniform;
+    double u_uniform[3];
+    double F[3];
+    double dt, rho0, scale;
+    int zero_walls;         // rho = u = 0 on wall nodes (initMethods.jl:622-624)
+    int force_mode;
+};
+
+// findInitialConditions (src/gpu/initMethods.jl:417-438):
+//   u' = u - dt/2 F/rho (F/rho = 0 where rho == 0), f_i = f_eq(rho, u')
+// evaluated in FP64 in the reference's operation order, then encoded.
+template <class L, int ST>
+__global__ void k_init(const InitArgs a) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    using R = typename SS::R;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    constexpr int D = L::D;
+    double rho = a.rho ? a.rho[c] : a.rho_uniform;
+    double u[3] = {0, 0, 0};
+    for (int k = 0; k < D; ++k) u[k] = a.u ? a.u[k * a.N + c] : a.u_uniform[k];
+    const bool w = a.wall && a.wall[c];
+    if (a.zero_walls && w) {
+        rho = 0.0;
+        u[0] = u[1] = u[2] = 0.0;
+    }
+    if (a.force_mode != 0) {
+        for (int k = 0; k < D; ++k) {
+            const double Fk = a.force_mode == 1 ? (w ? 0.0 : a.F[k]) : a.ffield[k * a.N + c];
+            const double cons = rho == 0.0 ? 0.0 : __ddiv_rn(Fk, rho);
+            u[k] = __dsub_rn(u[k], __dmul_rn(__dmul_rn(0.5, a.dt), cons));
+        }
+    }
+    double uu = 0.0;
+    for (int k = 0; k < D; ++k) uu = __dadd_rn(uu, __dmul_rn(u[k], u[k]));
+    T* pop = static_cast<T*>(a.pop);
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        double uc = 0.0;
+        uc = __dadd_rn(uc, __dmul_rn(u[0], (double)L::cx(i)));
+        uc = __dadd_rn(uc, __dmul_rn(u[1], (double)L::cy(i)));
+        if (D == 3) uc = __dadd_rn(uc, __dmul_rn(u[2], (double)L::cz(i)));
+        const double first = __dadd_rn(__dmul_rn(uc, 3.0), __dmul_rn(__dmul_rn(uc, uc), 4.5));
+        const double second = __dadd_rn(__dsub_rn(first, __dmul_rn(uu, 1.5)), 1.0);
+        const double f = __dmul_rn(second, __dmul_rn(L::w(i), rho));
+        const double g = f * (1.0 / L::w(i)) - a.rho0;
+        pop[i * a.N + c] = SS::enc((R)g, (R)a.scale);
+    }
+}
+
+struct MaskArgs {
+    unsigned char* mask;
+    const double* coord[3];
+    int n[3];
+    long long N;
+    double c[3];
+    double r2;
+};
+
+// getSphere over the whole grid (src/gpu/aux.jl:206-215)
+template <int D>
+__global__ void k_mask(const MaskArgs a) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= a.N) return;
+    const int x = (int)(q % a.n[0]);
+    const int y = (int)((q / a.n[0]) % a.n[1]);
+    const int z = (int)(q / ((long long)a.n[0] * a.n[1]));
+    a.mask[q] = sphere_test<D>(a.coord[0][x], a.coord[1][y], D == 3 ? a.coord[2][z] : 0.0, a.c, a.r2) ? 1 : 0;
+}
+
+// device-side scan for non-finite or non-positive densities (fault detection)
+template <class L, int ST>
+__global__ void k_check(const CodecArgs a, int* bad) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    if (a.wall && a.wall[c]) return;
+    const T* pop = static_cast<const T*>(a.pop);
+    double drho = 0;
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) drho += L::w(i) * (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale);
+    const double rho = a.rho0 + drho;
+    if (!(rho > 0.0) || !isfinite(rho)) atomicOr(bad, 1);
+}
+
+}  // namespace lbm

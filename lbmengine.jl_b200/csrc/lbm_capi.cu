@@ -1,0 +1,1093 @@
+// C ABI of the B200 lattice-Boltzmann library (include/lbm_b200.h).
+//
+// Host side of the drop-in boundary: validates the resolved modelInit /
+// addSquirmer! keyword sets, owns all device memory of a model, and runs
+// LBMpropagate! as CUDA-graph replays of the fused tick
+// (k_boundary || k_bulk) -> k_particles on one stream.
+#include "lbm_b200.h"
+#include "ops.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace lbm;
+
+namespace {
+
+thread_local std::string g_global_err;
+
+const char* kBuildInfo =
+    "lbm_b200: sm_100a fused push collide-stream (BGK/TRT + Guo), halfway bounce-back, "
+    "Ladd squirmer coupling; storage f32/f16/bf16/f64";
+
+struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    int start_buf = -1;
+};
+
+}  // namespace
+
+struct lbm_handle {
+    // configuration
+    int device = 0;
+    int dims = 0, q = 0, lattice = 0, storage = 0, trt = 0;
+    int n[3] = {1, 1, 1};
+    long long N = 0;
+    GridDesc g{};
+    double dx = 1, dt = 1, tau = 1, tau_minus = 1;
+    double rho0 = 1, scale = 1;
+    int force_mode = 0;
+    double F[3] = {0, 0, 0};
+    int incompressible = 0;
+    double rho_inc = 1;
+    bool has_walls = false, moving_walls = false;
+    std::vector<double> X[3];
+    Ops ops{};
+    // device state
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void* pop[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* d_coord[3] = {nullptr, nullptr, nullptr};
+    unsigned char* d_wall = nullptr;
+    double* d_uw = nullptr;
+    double* d_ffield = nullptr;
+    unsigned char* d_tileflags = nullptr;
+    int* d_walltiles = nullptr;
+    int nwalltiles = 0;
+    unsigned long long* d_tilebits = nullptr;
+    int words = 1;
+    ParticleDev* d_parts = nullptr;
+    int pcap = 0;
+    std::vector<ParticleDev> hparts;  // host copy of the static fields
+    double* d_partial = nullptr;
+    long long partial_slots = 0;
+    int maxtl = 0;
+    int* d_err = nullptr;
+    double* d_tmp = nullptr;  // FP64 read-back / upload scratch
+    size_t tmp_bytes = 0;
+    size_t device_bytes = 0;
+    // time
+    long long tick = 0;
+    double time = 0;
+    // graphs of kGraphSteps ticks, one per starting buffer; [1] with event nodes
+    Graph graphs[2][2];
+    // profiling: per graph slot, events before/after the bulk kernel, around the
+    // boundary kernel and after the particle kernel; plus the whole call
+    bool profiling = false;
+    std::vector<cudaEvent_t> pev;
+    cudaEvent_t t_begin = nullptr, t_end = nullptr;
+    lbm_profile prof{};
+    std::string err;
+};
+
+namespace {
+
+constexpr int kGraphSteps = 16;
+
+int set_err(lbm_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_global_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                              \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return set_err((h), e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,          \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+        }                                                                                              \
+    } while (0)
+
+// every entry point runs on the handle's device, whatever the caller's current device
+#define BIND(h)                                                                                        \
+    do {                                                                                               \
+        if (cudaSetDevice((h)->device) != cudaSuccess) {                                               \
+            cudaGetLastError();                                                                        \
+            return set_err((h), LBM_ERR_CUDA, "cannot select the handle's CUDA device");               \
+        }                                                                                              \
+    } while (0)
+
+template <class P>
+int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
+    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return set_err(h, LBM_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                                           cudaGetErrorString(e));
+    }
+    h->device_bytes += bytes;
+    return LBM_OK;
+}
+
+template <class P>
+void dev_free(P*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+bool get_ops(int lattice, int storage, int trt, Ops* o) {
+    switch (lattice) {
+        case LBM_D2Q9: return ops_d2q9(storage, trt, o);
+        case LBM_D3Q15: return ops_d3q15(storage, trt, o);
+        case LBM_D3Q19: return ops_d3q19(storage, trt, o);
+        case LBM_D3Q27: return ops_d3q27(storage, trt, o);
+        default: return false;
+    }
+}
+
+// host copy of the lattice (for link enumeration and checks)
+struct HostLattice {
+    int q = 0, d = 0;
+    std::vector<int> cx, cy, cz, opp;
+    std::vector<double> w;
+};
+
+template <class L>
+HostLattice host_lattice_of() {
+    HostLattice hl;
+    hl.q = L::Q;
+    hl.d = L::D;
+    for (int i = 0; i < L::Q; ++i) {
+        hl.cx.push_back(L::cx(i));
+        hl.cy.push_back(L::cy(i));
+        hl.cz.push_back(L::cz(i));
+        hl.opp.push_back(L::opp(i));
+        hl.w.push_back(L::w(i));
+    }
+    return hl;
+}
+
+HostLattice host_lattice(int lattice) {
+    switch (lattice) {
+        case LBM_D2Q9: return host_lattice_of<D2Q9>();
+        case LBM_D3Q15: return host_lattice_of<D3Q15>();
+        case LBM_D3Q19: return host_lattice_of<D3Q19>();
+        default: return host_lattice_of<D3Q27>();
+    }
+}
+
+int ensure_tmp(lbm_handle* h, size_t bytes) {
+    if (h->tmp_bytes >= bytes) return LBM_OK;
+    dev_free(h->d_tmp);
+    h->device_bytes -= h->tmp_bytes;
+    h->tmp_bytes = 0;
+    int rc = dev_alloc(h, &h->d_tmp, bytes);
+    if (rc) return rc;
+    h->tmp_bytes = bytes;
+    return LBM_OK;
+}
+
+void drop_graphs(lbm_handle* h) {
+    for (auto& row : h->graphs)
+        for (auto& gr : row) {
+            if (gr.exec) cudaGraphExecDestroy(gr.exec);
+            gr.exec = nullptr;
+            gr.start_buf = -1;
+        }
+}
+
+StepArgs step_args(const lbm_handle* h, int src) {
+    StepArgs a{};
+    a.src = h->pop[src];
+    a.dst = h->pop[1 - src];
+    a.g = h->g;
+    for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
+    a.tilebits = h->d_tilebits;
+    a.tileflags = h->d_tileflags;
+    a.walltiles = h->d_walltiles;
+    a.nwalltiles = h->nwalltiles;
+    a.words = h->words;
+    a.wall = h->d_wall;
+    a.uw = h->d_uw;
+    a.ffield = h->d_ffield;
+    a.parts = h->d_parts;
+    a.nparts = (int)h->hparts.size();
+    a.maxtl = h->maxtl;
+    a.partial = h->d_partial;
+    a.err = h->d_err;
+    a.rho0 = h->rho0;
+    a.scale = h->scale;
+    a.inv_scale = 1.0 / h->scale;
+    a.omega = h->dt / h->tau;
+    a.omega_p = h->dt / h->tau;
+    a.omega_m = h->trt ? h->dt / h->tau_minus : 0.0;
+    a.guo_k = h->dt * (1 - h->dt / (2 * h->tau));
+    a.guo_kp = a.guo_k;
+    a.guo_km = h->trt ? h->dt * (1 - h->dt / (2 * h->tau_minus)) : 0.0;
+    for (int k = 0; k < 3; ++k) a.F[k] = h->F[k];
+    a.half_dt = 0.5 * h->dt;
+    a.coeff = std::pow(h->dx, h->dims) / h->dt;
+    a.force_mode = h->force_mode;
+    a.incompressible = h->incompressible;
+    a.rho_inc = h->rho_inc;
+    return a;
+}
+
+ParticleArgs particle_args(const lbm_handle* h, int mode, int pid) {
+    ParticleArgs a{};
+    a.parts = h->d_parts;
+    a.nparts = (int)h->hparts.size();
+    a.mode = mode;
+    a.setup_pid = pid;
+    a.partial = h->d_partial;
+    a.tilebits = h->d_tilebits;
+    a.words = h->words;
+    a.g = h->g;
+    for (int k = 0; k < 3; ++k) {
+        a.coord[k] = h->d_coord[k];
+        a.x0[k] = h->X[k].empty() ? 0.0 : h->X[k][0];
+    }
+    a.dx = h->dx;
+    a.dt = h->dt;
+    a.err = h->d_err;
+    return a;
+}
+
+CodecArgs codec_args(const lbm_handle* h) {
+    CodecArgs c{};
+    c.pop = h->pop[h->cur];
+    c.N = h->N;
+    c.wall = h->d_wall;
+    c.ffield = h->d_ffield;
+    c.rho0 = h->rho0;
+    c.scale = h->scale;
+    c.inv_scale = 1.0 / h->scale;
+    c.half_dt = 0.5 * h->dt;
+    for (int k = 0; k < 3; ++k) c.F[k] = h->F[k];
+    c.force_mode = h->force_mode;
+    return c;
+}
+
+// events of graph slot s: [0] before bulk, [1] after bulk, [2] before boundary,
+// [3] after boundary, [4] after particles
+cudaEvent_t prof_event(lbm_handle* h, int slot, int k) { return h->pev[slot * 5 + k]; }
+
+void prof_record(lbm_handle* h, int slot, int k, cudaStream_t s) {
+    if (h->profiling) cudaEventRecordWithFlags(prof_event(h, slot, k), s, cudaEventRecordExternal);
+}
+
+// enqueue one tick on h->stream (capturable); `slot` selects the profiling events
+void enqueue_tick(lbm_handle* h, int src, int slot) {
+    const StepArgs a = step_args(h, src);
+    const dim3 block(h->g.t[0], h->g.t[1], h->g.t[2]);
+    const long long nb = (long long)a.nparts * a.maxtl + a.nwalltiles;
+    if (nb > 0) {
+        // boundary tiles on a side branch, concurrent with the bulk tiles
+        cudaEventRecord(h->ev_fork, h->stream);
+        cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+        prof_record(h, slot, 2, h->side);
+        h->ops.boundary(a, (unsigned)nb, block, h->side);
+        prof_record(h, slot, 3, h->side);
+        cudaEventRecord(h->ev_join, h->side);
+    }
+    prof_record(h, slot, 0, h->stream);
+    h->ops.bulk(a, (unsigned)h->g.ntiles, block, h->stream);
+    prof_record(h, slot, 1, h->stream);
+    if (nb > 0) cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    if (a.nparts > 0) h->ops.particles(particle_args(h, 0, 0), (unsigned)a.nparts, h->stream);
+    prof_record(h, slot, 4, h->stream);
+}
+
+int launches_per_tick(const lbm_handle* h) {
+    const long long nb = (long long)h->hparts.size() * h->maxtl + h->nwalltiles;
+    return 1 + (nb > 0 ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
+}
+
+int build_graph(lbm_handle* h, int start) {
+    Graph& gr = h->graphs[h->profiling ? 1 : 0][start];
+    if (gr.exec) return LBM_OK;
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int b = start;
+    for (int s = 0; s < kGraphSteps; ++s) {
+        enqueue_tick(h, b, s);
+        b = 1 - b;
+    }
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(h, LBM_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+    }
+    e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gr.exec = nullptr;
+        return set_err(h, LBM_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+    }
+    gr.start_buf = start;
+    return LBM_OK;
+}
+
+int check_device_error(lbm_handle* h) {
+    int err = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (err & kErrTooManyCandidates)
+        return set_err(h, LBM_ERR_UNSUPPORTED, "more than 16 particles meet one tile of the lattice");
+    if (err & kErrPartialOverflow) return set_err(h, LBM_ERR_STATE, "particle tile box exceeded its partial-sum capacity");
+    return LBM_OK;
+}
+
+// choose the CTA tile: full x-rows up to 256 nodes (x-wrap stays inside the CTA)
+void choose_tiles(lbm_handle* h) {
+    GridDesc& g = h->g;
+    for (int k = 0; k < 3; ++k) g.n[k] = h->n[k];
+    int t0 = std::min(256, ((h->n[0] + 31) / 32) * 32);
+    int t1 = std::max(1, std::min(256 / t0, h->n[1]));
+    // keep the CTA a multiple of 32 threads
+    g.t[0] = t0;
+    g.t[1] = t1;
+    g.t[2] = 1;
+    for (int k = 0; k < 3; ++k) g.nt[k] = (h->n[k] + g.t[k] - 1) / g.t[k];
+    g.N = h->N;
+    g.ntiles = (long long)g.nt[0] * g.nt[1] * g.nt[2];
+}
+
+int upload(lbm_handle* h, void* dst, const void* src, size_t bytes) {
+    CUDA_TRY(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    return LBM_OK;
+}
+
+void destroy_all(lbm_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
+    dev_free(h->pop[0]);
+    dev_free(h->pop[1]);
+    for (auto& c : h->d_coord) dev_free(c);
+    dev_free(h->d_wall);
+    dev_free(h->d_uw);
+    dev_free(h->d_ffield);
+    dev_free(h->d_tileflags);
+    dev_free(h->d_walltiles);
+    dev_free(h->d_tilebits);
+    dev_free(h->d_parts);
+    dev_free(h->d_partial);
+    dev_free(h->d_err);
+    dev_free(h->d_tmp);
+    for (auto& e : h->pev) cudaEventDestroy(e);
+    if (h->t_begin) cudaEventDestroy(h->t_begin);
+    if (h->t_end) cudaEventDestroy(h->t_end);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int storage_bytes(int storage) {
+    switch (storage) {
+        case LBM_STORE_F16:
+        case LBM_STORE_BF16: return 2;
+        case LBM_STORE_F64: return 8;
+        default: return 4;
+    }
+}
+
+// grow device particle storage / tile-bit words / partial-sum slots
+int ensure_particle_capacity(lbm_handle* h, int nparts_new, long long slots_new) {
+    if (nparts_new > h->pcap) {
+        int cap = std::max(8, h->pcap * 2);
+        while (cap < nparts_new) cap *= 2;
+        ParticleDev* np = nullptr;
+        int rc = dev_alloc(h, &np, sizeof(ParticleDev) * cap);
+        if (rc) return rc;
+        if (h->d_parts) {
+            CUDA_TRY(h, cudaMemcpyAsync(np, h->d_parts, sizeof(ParticleDev) * h->hparts.size(),
+                                        cudaMemcpyDeviceToDevice, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            dev_free(h->d_parts);
+        }
+        h->d_parts = np;
+        h->pcap = cap;
+    }
+    int words_new = (nparts_new + 63) / 64;
+    if (words_new > h->words || !h->d_tilebits) {
+        int w = std::max(words_new, h->words);
+        unsigned long long* nb = nullptr;
+        int rc = dev_alloc(h, &nb, sizeof(unsigned long long) * h->g.ntiles * w);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaMemsetAsync(nb, 0, sizeof(unsigned long long) * h->g.ntiles * w, h->stream));
+        if (h->d_tilebits) {
+            CUDA_TRY(h, cudaMemcpy2DAsync(nb, sizeof(unsigned long long) * w, h->d_tilebits,
+                                          sizeof(unsigned long long) * h->words,
+                                          sizeof(unsigned long long) * h->words, h->g.ntiles,
+                                          cudaMemcpyDeviceToDevice, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            dev_free(h->d_tilebits);
+        }
+        h->d_tilebits = nb;
+        h->words = w;
+    }
+    if (slots_new > h->partial_slots) {
+        dev_free(h->d_partial);
+        int rc = dev_alloc(h, &h->d_partial, sizeof(double) * kPartialStride * slots_new);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaMemsetAsync(h->d_partial, 0, sizeof(double) * kPartialStride * slots_new, h->stream));
+        h->partial_slots = slots_new;
+    }
+    return LBM_OK;
+}
+
+bool is_uniform_axis(const std::vector<double>& X, double dx) {
+    for (size_t i = 1; i < X.size(); ++i) {
+        const double expect = X[0] + (double)i * dx;
+        if (std::fabs(X[i] - expect) > 1e-9 * (std::fabs(expect) + std::fabs(dx) + 1.0)) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t lbm_abi_version(void) { return LBM_ABI_VERSION; }
+const char* lbm_build_info(void) { return kBuildInfo; }
+const char* lbm_last_global_error(void) { return g_global_err.c_str(); }
+const char* lbm_last_error(lbm_handle* h) { return h ? h->err.c_str() : g_global_err.c_str(); }
+
+int lbm_create(const lbm_config* cfg, lbm_handle** out) {
+    if (!cfg || !out) return set_err(nullptr, LBM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(nullptr, LBM_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    int device = cfg->device;
+    if (device >= ndev) return set_err(nullptr, LBM_ERR_INVALID, "no CUDA device with that ordinal");
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) return set_err(nullptr, LBM_ERR_CUDA, "cudaGetDevice failed");
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(nullptr, LBM_ERR_CUDA, "cudaSetDevice failed");
+    }
+    if (cfg->dims != 2 && cfg->dims != 3) return set_err(nullptr, LBM_ERR_INVALID, "dims must be 2 or 3");
+    const int vd = cfg->lattice == LBM_D2Q9 ? 2 : 3;
+    if (cfg->lattice != LBM_D2Q9 && cfg->lattice != LBM_D3Q15 && cfg->lattice != LBM_D3Q19 &&
+        cfg->lattice != LBM_D3Q27)
+        return set_err(nullptr, LBM_ERR_INVALID,
+                       "If a default velocity set is chosen, it must be one of the following: [:D2Q9, :D3Q15, :D3Q19, :D3Q27]");
+    if (vd != cfg->dims)
+        return set_err(nullptr, LBM_ERR_INVALID,
+                       "The chosen velocity must be " + std::to_string(cfg->dims) + "-dimensional!");
+    if (cfg->collision != LBM_BGK && cfg->collision != LBM_TRT)
+        return set_err(nullptr, LBM_ERR_INVALID, "Collision model is not implemented!");
+    if (cfg->storage < LBM_STORE_F32 || cfg->storage > LBM_STORE_F64)
+        return set_err(nullptr, LBM_ERR_INVALID, "unknown storage format");
+    if (!(cfg->dx > 0) || !std::isfinite(cfg->dx)) return set_err(nullptr, LBM_ERR_INVALID, "latticeParameter must be positive");
+    if (!(cfg->tau > 0.5 * cfg->dx)) return set_err(nullptr, LBM_ERR_INVALID, "relaxation time must exceed dt/2");
+    if (cfg->collision == LBM_TRT && !(cfg->tau_minus > 0.5 * cfg->dx))
+        return set_err(nullptr, LBM_ERR_INVALID, "TRT tau- must exceed dt/2");
+    long long N = 1;
+    for (int a = 0; a < 3; ++a) {
+        const long long na = a < cfg->dims ? cfg->n[a] : 1;
+        if (na < 1 || na > (1 << 20)) return set_err(nullptr, LBM_ERR_INVALID, "grid sizes must be in [1, 2^20]");
+        N *= na;
+    }
+    if (N >= (1LL << 31)) return set_err(nullptr, LBM_ERR_UNSUPPORTED, "more than 2^31 lattice nodes");
+    if (cfg->force_mode < LBM_FORCE_NONE || cfg->force_mode > LBM_FORCE_FIELD)
+        return set_err(nullptr, LBM_ERR_INVALID, "unknown force mode");
+    if (cfg->force_mode == LBM_FORCE_FIELD && !cfg->force_field)
+        return set_err(nullptr, LBM_ERR_INVALID, "force density does not have consistent dimensions!");
+    if (!cfg->compressible && cfg->rho_init)
+        return set_err(nullptr, LBM_ERR_UNSUPPORTED, "incompressible equilibrium with a non-uniform initial density");
+
+    lbm_handle* h = new lbm_handle();
+    h->device = device;
+    h->dims = cfg->dims;
+    h->lattice = cfg->lattice;
+    h->q = cfg->lattice;
+    h->storage = cfg->storage;
+    h->trt = cfg->collision == LBM_TRT;
+    for (int a = 0; a < 3; ++a) h->n[a] = a < cfg->dims ? (int)cfg->n[a] : 1;
+    h->N = N;
+    h->dx = cfg->dx;
+    h->dt = cfg->dx;
+    h->tau = cfg->tau;
+    h->tau_minus = cfg->tau_minus;
+    h->rho0 = cfg->rho_ref > 0 ? cfg->rho_ref : 1.0;
+    h->scale = (cfg->storage == LBM_STORE_F16 || cfg->storage == LBM_STORE_BF16)
+                   ? (cfg->store_scale > 0 ? cfg->store_scale : 4096.0)
+                   : 1.0;
+    h->force_mode = cfg->force_mode;
+    if (cfg->force_mode == LBM_FORCE_UNIFORM)
+        for (int k = 0; k < cfg->dims; ++k) h->F[k] = cfg->force[k];
+    h->incompressible = cfg->compressible ? 0 : 1;
+    h->rho_inc = cfg->rho_uniform;
+    if (!get_ops(h->lattice, h->storage, h->trt, &h->ops)) {
+        delete h;
+        return set_err(nullptr, LBM_ERR_INVALID, "no kernel instantiation for this configuration");
+    }
+    for (int a = 0; a < 3; ++a) {
+        h->X[a].resize(h->n[a]);
+        for (int i = 0; i < h->n[a]; ++i)
+            h->X[a][i] = (a < cfg->dims && cfg->coords[a]) ? cfg->coords[a][i] : cfg->x0[a] + (double)i * h->dx;
+        if (a < cfg->dims && !is_uniform_axis(h->X[a], h->dx)) {
+            delete h;
+            return set_err(nullptr, LBM_ERR_INVALID, "node coordinates must form a uniform grid with spacing dx");
+        }
+    }
+    choose_tiles(h);
+    int rc = LBM_OK;
+#define TRY(x)                       \
+    do {                             \
+        rc = (x);                    \
+        if (rc != LBM_OK) {          \
+            g_global_err = h->err;   \
+            destroy_all(h);          \
+            return rc;               \
+        }                            \
+    } while (0)
+    TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess
+            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
+    TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) == cudaSuccess
+            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
+    TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess
+            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "event creation failed"));
+    TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) == cudaSuccess
+            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "event creation failed"));
+    const size_t pop_bytes = (size_t)N * h->q * storage_bytes(h->storage);
+    TRY(dev_alloc(h, &h->pop[0], pop_bytes));
+    TRY(dev_alloc(h, &h->pop[1], pop_bytes));
+    for (int a = 0; a < 3; ++a) {
+        TRY(dev_alloc(h, &h->d_coord[a], sizeof(double) * h->n[a]));
+        TRY(upload(h, h->d_coord[a], h->X[a].data(), sizeof(double) * h->n[a]));
+    }
+    TRY(dev_alloc(h, &h->d_err, sizeof(int)));
+    CUDA_TRY(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+
+    // walls (initMethods.jl:568-628): mask | {|u_w| > 0}
+    std::vector<unsigned char> W;
+    if (cfg->wall_mask || cfg->wall_velocity) {
+        W.assign(N, 0);
+        if (cfg->wall_mask)
+            for (long long c = 0; c < N; ++c) W[c] = cfg->wall_mask[c] ? 1 : 0;
+        if (cfg->wall_velocity) {
+            for (long long c = 0; c < N; ++c)
+                for (int k = 0; k < h->dims; ++k)
+                    if (cfg->wall_velocity[k * N + c] != 0.0) W[c] = 1;
+            h->moving_walls = true;
+            TRY(dev_alloc(h, &h->d_uw, sizeof(double) * N * h->dims));
+            TRY(upload(h, h->d_uw, cfg->wall_velocity, sizeof(double) * N * h->dims));
+        }
+        h->has_walls = true;
+        TRY(dev_alloc(h, &h->d_wall, N));
+        TRY(upload(h, h->d_wall, W.data(), N));
+    }
+    // tiles whose halo meets a wall node
+    std::vector<unsigned char> tflags(h->g.ntiles, 0);
+    std::vector<int> wtiles;
+    if (h->has_walls) {
+        const GridDesc& g = h->g;
+        for (int z = 0; z < h->n[2]; ++z)
+            for (int y = 0; y < h->n[1]; ++y)
+                for (int x = 0; x < h->n[0]; ++x) {
+                    if (!W[x + (long long)h->n[0] * (y + (long long)h->n[1] * z)]) continue;
+                    for (int dz = -1; dz <= 1; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dxx = -1; dxx <= 1; ++dxx) {
+                                if (h->dims == 2 && dz != 0) continue;
+                                const int xx = (x + dxx + h->n[0]) % h->n[0];
+                                const int yy = (y + dy + h->n[1]) % h->n[1];
+                                const int zz = (z + dz + h->n[2]) % h->n[2];
+                                const long long t = xx / g.t[0] + (long long)g.nt[0] * (yy / g.t[1] + (long long)g.nt[1] * (zz / g.t[2]));
+                                tflags[t] = 1;
+                            }
+                }
+        for (long long t = 0; t < g.ntiles; ++t)
+            if (tflags[t]) wtiles.push_back((int)t);
+    }
+    h->nwalltiles = (int)wtiles.size();
+    TRY(dev_alloc(h, &h->d_tileflags, h->g.ntiles));
+    TRY(upload(h, h->d_tileflags, tflags.data(), h->g.ntiles));
+    TRY(dev_alloc(h, &h->d_walltiles, sizeof(int) * std::max<size_t>(1, wtiles.size())));
+    if (!wtiles.empty()) TRY(upload(h, h->d_walltiles, wtiles.data(), sizeof(int) * wtiles.size()));
+    TRY(ensure_particle_capacity(h, 0, 0));
+
+    // force field, zeroed on walls (initMethods.jl:639-650)
+    std::vector<double> ff;
+    if (cfg->force_mode == LBM_FORCE_FIELD) {
+        ff.assign(cfg->force_field, cfg->force_field + N * h->dims);
+        if (h->has_walls)
+            for (int k = 0; k < h->dims; ++k)
+                for (long long c = 0; c < N; ++c)
+                    if (W[c]) ff[k * N + c] = 0.0;
+        TRY(dev_alloc(h, &h->d_ffield, sizeof(double) * N * h->dims));
+        TRY(upload(h, h->d_ffield, ff.data(), sizeof(double) * N * h->dims));
+    }
+    // initial populations on the device (findInitialConditions)
+    size_t need = 0;
+    if (cfg->rho_init) need += sizeof(double) * N;
+    if (cfg->u_init) need += sizeof(double) * N * h->dims;
+    if (need) TRY(ensure_tmp(h, need));
+    InitArgs ia{};
+    ia.pop = h->pop[0];
+    ia.N = N;
+    double* tp = h->d_tmp;
+    if (cfg->rho_init) {
+        TRY(upload(h, tp, cfg->rho_init, sizeof(double) * N));
+        ia.rho = tp;
+        tp += N;
+    }
+    if (cfg->u_init) {
+        TRY(upload(h, tp, cfg->u_init, sizeof(double) * N * h->dims));
+        ia.u = tp;
+    }
+    ia.wall = h->d_wall;
+    ia.ffield = h->d_ffield;
+    ia.rho_uniform = cfg->rho_uniform;
+    for (int k = 0; k < 3; ++k) {
+        ia.u_uniform[k] = cfg->u_uniform[k];
+        ia.F[k] = h->F[k];
+    }
+    ia.dt = h->dt;
+    ia.rho0 = h->rho0;
+    ia.scale = h->scale;
+    ia.zero_walls = (h->has_walls || h->trt) ? 1 : 0;
+    ia.force_mode = h->force_mode;
+    h->ops.init(ia, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemsetAsync(h->pop[1], 0, pop_bytes, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+#undef TRY
+    h->cur = 0;
+    *out = h;
+    return LBM_OK;
+}
+
+int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_out) {
+    if (!h || !p) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    if (p->kind != LBM_BEAD && p->kind != LBM_SQUIRMER) return set_err(h, LBM_ERR_INVALID, "unknown particle kind");
+    if ((int)h->hparts.size() >= 255)
+        return set_err(h, LBM_ERR_INVALID, "particle ids are UInt8 in the reference: at most 255 particles");
+    if (!(p->radius > 0) || !std::isfinite(p->radius)) return set_err(h, LBM_ERR_INVALID, "radius must be positive");
+    const int d = h->dims;
+    // mass (initMethods.jl:18/108): node count of the origin-centred sphere
+    const double r2 = p->radius * p->radius;
+    long long count = 0;
+    {
+        std::vector<int> ax[3];
+        for (int a = 0; a < 3; ++a) {
+            if (a >= d) {
+                ax[a].push_back(0);
+                continue;
+            }
+            for (int i = 0; i < h->n[a]; ++i) {
+                const double v = h->X[a][i];
+                if (v * v < r2) ax[a].push_back(i);
+            }
+        }
+        for (int z : ax[2])
+            for (int y : ax[1])
+                for (int x : ax[0]) {
+                    const double a0 = h->X[0][x], a1 = h->X[1][y];
+                    volatile double s = a0 * a0;
+                    volatile double t1 = a1 * a1;
+                    double s2 = s + t1;
+                    if (d == 3) {
+                        const double a2 = h->X[2][z];
+                        volatile double t2 = a2 * a2;
+                        s2 = s2 + t2;
+                    }
+                    if (s2 < r2) ++count;
+                }
+    }
+    const double mass = p->mass_density * (double)count * std::pow(h->dx, d);
+    const double inertia = d == 2 ? 0.5 * mass * r2 : 0.4 * mass * r2;
+    ParticleDev P{};
+    for (int k = 0; k < 3; ++k) {
+        P.R[k] = k < d ? p->position[k] : 0.0;
+        P.v[k] = k < d ? p->velocity[k] : 0.0;
+        P.w[k] = d == 2 ? (k == 0 ? p->angular_velocity[0] : 0.0) : p->angular_velocity[k];
+        P.e[k] = (p->kind == LBM_SQUIRMER && k < d) ? p->swimming_direction[k] : 0.0;
+    }
+    P.radius = p->radius;
+    P.r2 = r2;
+    P.B1 = p->kind == LBM_SQUIRMER ? p->B1 : 0.0;
+    P.B2 = p->kind == LBM_SQUIRMER ? p->B2 : 0.0;
+    P.inv_mass = 1.0 / mass;
+    P.inv_inertia = 1.0 / inertia;
+    P.kind = p->kind;
+    P.coupleF = p->couple_forces ? 1 : 0;
+    P.coupleT = p->couple_torques ? 1 : 0;
+    P.valid = 0;
+    // partial-sum capacity: tiles covering the widest node box of the sphere
+    int cap = 1;
+    for (int a = 0; a < 3; ++a) {
+        int ta;
+        if (a >= d) {
+            ta = 1;
+        } else {
+            const int span = (int)std::floor(2.0 * p->radius / h->dx) + 8;
+            ta = std::min(h->g.nt[a], (span + h->g.t[a] - 1) / h->g.t[a] + 1);
+        }
+        cap *= ta;
+    }
+    long long off = 0;
+    for (const auto& q : h->hparts) off = std::max<long long>(off, (long long)q.part_off + q.part_cap);
+    P.part_off = (int)off;
+    P.part_cap = cap;
+    const int pid = (int)h->hparts.size();
+    int rc = ensure_particle_capacity(h, pid + 1, off + cap);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_parts + pid, &P, sizeof(P), cudaMemcpyHostToDevice, h->stream));
+    h->hparts.push_back(P);
+    h->maxtl = std::max(h->maxtl, cap);
+    drop_graphs(h);
+    // initial setup: moveParticles!(initialSetup = true)
+    h->ops.particles(particle_args(h, 1, pid), 1, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    rc = check_device_error(h);
+    if (rc) return rc;
+    if (id_out) *id_out = pid + 1;
+    return LBM_OK;
+}
+
+int lbm_step(lbm_handle* h, int64_t nsteps) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (nsteps < 0) return set_err(h, LBM_ERR_INVALID, "ticks must be non-negative");
+    BIND(h);
+    if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_begin, h->stream));
+    int64_t done = 0;
+    int slots_used = 0;
+    while (nsteps - done >= kGraphSteps) {
+        int rc = build_graph(h, h->cur);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling ? 1 : 0][h->cur].exec, h->stream));
+        done += kGraphSteps;  // kGraphSteps is even: the buffer parity is unchanged
+        slots_used = kGraphSteps;
+    }
+    for (int s = 0; done < nsteps; ++done, ++s) {
+        enqueue_tick(h, h->cur, s % kGraphSteps);
+        h->cur = 1 - h->cur;
+        slots_used = std::max(slots_used, std::min(s + 1, kGraphSteps));
+    }
+    if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_end, h->stream));
+    CUDA_TRY(h, cudaGetLastError());
+    for (int64_t s = 0; s < nsteps; ++s) h->time += h->dt;
+    h->tick += nsteps;
+    int rc = check_device_error(h);
+    lbm_profile& p = h->prof;
+    p = lbm_profile{};
+    p.steps = nsteps;
+    p.launches = nsteps * launches_per_tick(h);
+    if (h->profiling && nsteps > 0) {
+        float ms = 0;
+        CUDA_TRY(h, cudaEventElapsedTime(&ms, h->t_begin, h->t_end));
+        p.total_ms = ms;
+        const bool boundary = (long long)h->hparts.size() * h->maxtl + h->nwalltiles > 0;
+        double sb = 0, sbd = 0, sp = 0;
+        for (int s = 0; s < slots_used; ++s) {
+            CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 0), prof_event(h, s, 1)));
+            sb += ms;
+            if (boundary) {
+                CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 2), prof_event(h, s, 3)));
+                sbd += ms;
+            }
+            if (!h->hparts.empty()) {
+                // the particle kernel starts once both bulk and boundary have finished
+                float a = 0, b = 0;
+                CUDA_TRY(h, cudaEventElapsedTime(&a, prof_event(h, s, 1), prof_event(h, s, 4)));
+                if (boundary) CUDA_TRY(h, cudaEventElapsedTime(&b, prof_event(h, s, 3), prof_event(h, s, 4)));
+                sp += boundary ? std::min(a, b) : a;
+            }
+        }
+        p.bulk_ms = sb / slots_used;
+        p.boundary_ms = sbd / slots_used;
+        p.particles_ms = sp / slots_used;
+        p.profiled_steps = slots_used;
+        // tiles the bulk kernel skipped in the last tick (particle bits or wall flags)
+        std::vector<unsigned long long> bits((size_t)h->g.ntiles * h->words);
+        std::vector<unsigned char> flags(h->g.ntiles);
+        CUDA_TRY(h, cudaMemcpy(bits.data(), h->d_tilebits, bits.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(flags.data(), h->d_tileflags, flags.size(), cudaMemcpyDeviceToHost));
+        long long bcells = 0, btiles = 0;
+        const GridDesc& g = h->g;
+        for (long long t = 0; t < g.ntiles; ++t) {
+            bool b = flags[t] != 0;
+            for (int k = 0; k < h->words; ++k) b = b || bits[t * h->words + k] != 0;
+            if (!b) continue;
+            ++btiles;
+            const int tx = (int)(t % g.nt[0]), ty = (int)((t / g.nt[0]) % g.nt[1]), tz = (int)(t / ((long long)g.nt[0] * g.nt[1]));
+            const long long cx = std::min(g.t[0], g.n[0] - tx * g.t[0]);
+            const long long cy = std::min(g.t[1], g.n[1] - ty * g.t[1]);
+            const long long cz = std::min(g.t[2], g.n[2] - tz * g.t[2]);
+            bcells += cx * cy * cz;
+        }
+        p.bulk_cells = h->N - bcells;
+        p.boundary_tiles = btiles;
+    }
+    return rc;
+}
+
+int lbm_set_profiling(lbm_handle* h, int32_t on) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    BIND(h);
+    if (on && h->pev.empty()) {
+        h->pev.resize(5 * kGraphSteps);
+        for (auto& e : h->pev) CUDA_TRY(h, cudaEventCreate(&e));
+        CUDA_TRY(h, cudaEventCreate(&h->t_begin));
+        CUDA_TRY(h, cudaEventCreate(&h->t_end));
+    }
+    h->profiling = on != 0;
+    return LBM_OK;
+}
+
+int lbm_get_profile(lbm_handle* h, lbm_profile* out) {
+    if (!h || !out) return set_err(h, LBM_ERR_INVALID, "null argument");
+    *out = h->prof;
+    return LBM_OK;
+}
+
+int lbm_get_fields(lbm_handle* h, double* rho, double* u) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    BIND(h);
+    const size_t nb = sizeof(double) * h->N * (1 + h->dims);
+    int rc = ensure_tmp(h, nb);
+    if (rc) return rc;
+    CodecArgs c = codec_args(h);
+    c.rho = h->d_tmp;
+    c.u = h->d_tmp + h->N;
+    h->ops.macro(c, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, c.rho, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
+    if (u) CUDA_TRY(h, cudaMemcpyAsync(u, c.u, sizeof(double) * h->N * h->dims, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_get_distributions(lbm_handle* h, double* f) {
+    if (!h || !f) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    const size_t nb = sizeof(double) * h->N * h->q;
+    int rc = ensure_tmp(h, nb);
+    if (rc) return rc;
+    CodecArgs c = codec_args(h);
+    c.f64 = h->d_tmp;
+    h->ops.decode(c, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(f, c.f64, nb, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_set_distributions(lbm_handle* h, const double* f) {
+    if (!h || !f) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    const size_t nb = sizeof(double) * h->N * h->q;
+    int rc = ensure_tmp(h, nb);
+    if (rc) return rc;
+    CodecArgs c = codec_args(h);
+    c.f64 = h->d_tmp;
+    CUDA_TRY(h, cudaMemcpyAsync(c.f64, f, nb, cudaMemcpyHostToDevice, h->stream));
+    h->ops.encode(c, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_get_particles(lbm_handle* h, lbm_particle_state* out, int32_t capacity, int32_t* count) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    BIND(h);
+    const int np = (int)h->hparts.size();
+    if (count) *count = np;
+    if (!out || capacity <= 0 || np == 0) return LBM_OK;
+    std::vector<ParticleDev> tmp(np);
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->d_parts, sizeof(ParticleDev) * np, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < np && i < capacity; ++i) {
+        const ParticleDev& P = tmp[i];
+        lbm_particle_state& s = out[i];
+        std::memset(&s, 0, sizeof(s));
+        s.id = i + 1;
+        s.kind = P.kind;
+        s.couple_forces = P.coupleF;
+        s.couple_torques = P.coupleT;
+        s.radius = P.radius;
+        s.inverse_mass = P.inv_mass;
+        s.inverse_inertia = P.inv_inertia;
+        s.B1 = P.B1;
+        s.B2 = P.B2;
+        for (int k = 0; k < 3; ++k) {
+            s.position[k] = P.R[k];
+            s.velocity[k] = P.v[k];
+            s.angular_velocity[k] = P.w[k];
+            s.swimming_direction[k] = P.e[k];
+            s.last_force[k] = P.lastF[k];
+            s.last_torque[k] = P.lastT[k];
+        }
+    }
+    return LBM_OK;
+}
+
+int lbm_set_particle(lbm_handle* h, int32_t id, const lbm_particle_state* s) {
+    if (!h || !s) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    if (id < 1 || id > (int)h->hparts.size()) return set_err(h, LBM_ERR_INVALID, "no such particle");
+    ParticleDev P;
+    CUDA_TRY(h, cudaMemcpyAsync(&P, h->d_parts + (id - 1), sizeof(P), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < 3; ++k) {
+        P.R[k] = s->position[k];
+        P.v[k] = s->velocity[k];
+        P.w[k] = s->angular_velocity[k];
+        P.e[k] = s->swimming_direction[k];
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_parts + (id - 1), &P, sizeof(P), cudaMemcpyHostToDevice, h->stream));
+    h->ops.particles(particle_args(h, 1, id - 1), 1, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    return check_device_error(h);
+}
+
+int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask) {
+    if (!h || !mask) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    if (id < 1 || id > (int)h->hparts.size()) return set_err(h, LBM_ERR_INVALID, "no such particle");
+    ParticleDev P;
+    CUDA_TRY(h, cudaMemcpyAsync(&P, h->d_parts + (id - 1), sizeof(P), cudaMemcpyDeviceToHost, h->stream));
+    int rc = ensure_tmp(h, h->N);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    MaskArgs m{};
+    m.mask = reinterpret_cast<unsigned char*>(h->d_tmp);
+    for (int k = 0; k < 3; ++k) {
+        m.coord[k] = h->d_coord[k];
+        m.n[k] = h->n[k];
+        m.c[k] = P.mR[k];
+    }
+    m.N = h->N;
+    m.r2 = P.r2;
+    h->ops.mask(m, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(mask, m.mask, h->N, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_get_links(lbm_handle* h, int32_t id, int64_t* cells, int8_t* dirs, int64_t capacity, int64_t* n) {
+    if (!h || !n) return set_err(h, LBM_ERR_INVALID, "null argument");
+    std::vector<uint8_t> S(h->N);
+    int rc = lbm_get_mask(h, id, S.data());
+    if (rc) return rc;
+    const HostLattice hl = host_lattice(h->lattice);
+    std::vector<std::vector<int64_t>> per(hl.q);
+    for (long long y = 0; y < h->N; ++y) {
+        if (!S[y]) continue;
+        const int x0 = (int)(y % h->n[0]), y0 = (int)((y / h->n[0]) % h->n[1]), z0 = (int)(y / ((long long)h->n[0] * h->n[1]));
+        for (int i = 1; i < hl.q; ++i) {
+            const int xx = (x0 + hl.cx[i] + h->n[0]) % h->n[0];
+            const int yy = (y0 + hl.cy[i] + h->n[1]) % h->n[1];
+            const int zz = (z0 + hl.cz[i] + h->n[2]) % h->n[2];
+            const long long x = xx + (long long)h->n[0] * (yy + (long long)h->n[1] * zz);
+            if (!S[x]) per[i].push_back(x);
+        }
+    }
+    int64_t k = 0;
+    for (int i = 0; i < hl.q; ++i) {
+        std::sort(per[i].begin(), per[i].end());
+        for (int64_t x : per[i]) {
+            if (cells && dirs && k < capacity) {
+                cells[k] = x;
+                dirs[k] = (int8_t)i;
+            }
+            ++k;
+        }
+    }
+    *n = k;
+    return LBM_OK;
+}
+
+int lbm_get_info(lbm_handle* h, lbm_info* info) {
+    if (!h || !info) return set_err(h, LBM_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->dims = h->dims;
+    info->lattice = h->lattice;
+    info->q = h->q;
+    info->storage = h->storage;
+    for (int a = 0; a < 3; ++a) info->n[a] = h->n[a];
+    info->cells = h->N;
+    info->tick = h->tick;
+    info->time = h->time;
+    info->num_particles = (int32_t)h->hparts.size();
+    info->bytes_per_population = storage_bytes(h->storage);
+    info->device_bytes = (int64_t)h->device_bytes;
+    return LBM_OK;
+}
+
+// checkpoint: magic, header ints, tick/time, raw populations, particle records
+int lbm_save_state(lbm_handle* h, const char* path) {
+    if (!h || !path) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    const size_t pop_bytes = (size_t)h->N * h->q * storage_bytes(h->storage);
+    std::vector<char> buf(pop_bytes);
+    CUDA_TRY(h, cudaMemcpyAsync(buf.data(), h->pop[h->cur], pop_bytes, cudaMemcpyDeviceToHost, h->stream));
+    const int np = (int)h->hparts.size();
+    std::vector<ParticleDev> parts(np);
+    if (np) CUDA_TRY(h, cudaMemcpyAsync(parts.data(), h->d_parts, sizeof(ParticleDev) * np, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return set_err(h, LBM_ERR_INVALID, std::string("cannot open ") + path);
+    const int32_t hdr[8] = {0x4c424d42, LBM_ABI_VERSION, h->lattice, h->storage, h->n[0], h->n[1], h->n[2], np};
+    bool ok = std::fwrite(hdr, sizeof(hdr), 1, fp) == 1;
+    ok = ok && std::fwrite(&h->tick, sizeof(h->tick), 1, fp) == 1;
+    ok = ok && std::fwrite(&h->time, sizeof(h->time), 1, fp) == 1;
+    ok = ok && std::fwrite(buf.data(), 1, pop_bytes, fp) == pop_bytes;
+    if (np) ok = ok && std::fwrite(parts.data(), sizeof(ParticleDev), np, fp) == (size_t)np;
+    std::fclose(fp);
+    return ok ? LBM_OK : set_err(h, LBM_ERR_INVALID, "short write");
+}
+
+int lbm_load_state(lbm_handle* h, const char* path) {
+    if (!h || !path) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return set_err(h, LBM_ERR_INVALID, std::string("cannot open ") + path);
+    int32_t hdr[8];
+    bool ok = std::fread(hdr, sizeof(hdr), 1, fp) == 1;
+    const int np = (int)h->hparts.size();
+    if (!ok || hdr[0] != 0x4c424d42 || hdr[2] != h->lattice || hdr[3] != h->storage || hdr[4] != h->n[0] ||
+        hdr[5] != h->n[1] || hdr[6] != h->n[2] || hdr[7] != np) {
+        std::fclose(fp);
+        return set_err(h, LBM_ERR_INVALID, "checkpoint does not match this model (lattice, storage, grid, particles)");
+    }
+    long long tick = 0;
+    double time = 0;
+    const size_t pop_bytes = (size_t)h->N * h->q * storage_bytes(h->storage);
+    std::vector<char> buf(pop_bytes);
+    std::vector<ParticleDev> parts(np);
+    ok = std::fread(&tick, sizeof(tick), 1, fp) == 1 && std::fread(&time, sizeof(time), 1, fp) == 1 &&
+         std::fread(buf.data(), 1, pop_bytes, fp) == pop_bytes &&
+         (np == 0 || std::fread(parts.data(), sizeof(ParticleDev), np, fp) == (size_t)np);
+    std::fclose(fp);
+    if (!ok) return set_err(h, LBM_ERR_INVALID, "truncated checkpoint");
+    // clear the tile bits of the current geometry, then restore
+    CUDA_TRY(h, cudaMemsetAsync(h->d_tilebits, 0, sizeof(unsigned long long) * h->g.ntiles * h->words, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->pop[h->cur], buf.data(), pop_bytes, cudaMemcpyHostToDevice, h->stream));
+    for (int i = 0; i < np; ++i) {
+        parts[i].part_off = h->hparts[i].part_off;
+        parts[i].part_cap = h->hparts[i].part_cap;
+        parts[i].valid = 0;
+    }
+    if (np) CUDA_TRY(h, cudaMemcpyAsync(h->d_parts, parts.data(), sizeof(ParticleDev) * np, cudaMemcpyHostToDevice, h->stream));
+    // re-voxelise from the restored state; the slip snapshot is restored as saved
+    for (int i = 0; i < np; ++i) h->ops.particles(particle_args(h, 2, i), 1, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    h->tick = tick;
+    h->time = time;
+    return check_device_error(h);
+}
+
+void lbm_destroy(lbm_handle* h) { destroy_all(h); }
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// Launch table: one entry per (velocity set, storage, collision) instantiation.
+#pragma once
+#include <cuda_runtime.h>
+#include "kernels.cuh"
+#include "particles.cuh"
+#include "aux_kernels.cuh"
+
+namespace lbm {
+
+struct Ops {
+    void (*bulk)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
+    void (*boundary)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
+    void (*particles)(const ParticleArgs&, unsigned grid, cudaStream_t);
+    void (*encode)(const CodecArgs&, cudaStream_t);
+    void (*decode)(const CodecArgs&, cudaStream_t);
+    void (*macro)(const CodecArgs&, cudaStream_t);
+    void (*check)(const CodecArgs&, int*, cudaStream_t);
+    void (*init)(const InitArgs&, cudaStream_t);
+    void (*mask)(const MaskArgs&, cudaStream_t);
+    const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
+    const void* boundary_fn;
+};
+
+inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+template <class L, int ST, bool TRT>
+struct OpsImpl {
+    static void bulk(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
+        k_bulk<L, ST, TRT><<<grid, block, 0, s>>>(a);
+    }
+    static void boundary(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
+        k_boundary<L, ST, TRT><<<grid, block, 0, s>>>(a);
+    }
+    static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
+        k_particles<L><<<grid, 256, 0, s>>>(a);
+    }
+    static void encode(const CodecArgs& a, cudaStream_t s) { k_encode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static void macro(const CodecArgs& a, cudaStream_t s) { k_macro<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static void check(const CodecArgs& a, int* bad, cudaStream_t s) {
+        k_check<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a, bad);
+    }
+    static void init(const InitArgs& a, cudaStream_t s) { k_init<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static void mask(const MaskArgs& a, cudaStream_t s) { k_mask<L::D><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static Ops make() {
+        Ops o;
+        o.bulk = bulk;
+        o.boundary = boundary;
+        o.particles = particles;
+        o.encode = encode;
+        o.decode = decode;
+        o.macro = macro;
+        o.check = check;
+        o.init = init;
+        o.mask = mask;
+        o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
+        o.boundary_fn = (const void*)k_boundary<L, ST, TRT>;
+        return o;
+    }
+};
+
+template <class L>
+bool ops_for(int storage, int trt, Ops* out) {
+    switch (storage * 2 + (trt ? 1 : 0)) {
+        case ST_F32 * 2: *out = OpsImpl<L, ST_F32, false>::make(); return true;
+        case ST_F32 * 2 + 1: *out = OpsImpl<L, ST_F32, true>::make(); return true;
+        case ST_F16 * 2: *out = OpsImpl<L, ST_F16, false>::make(); return true;
+        case ST_F16 * 2 + 1: *out = OpsImpl<L, ST_F16, true>::make(); return true;
+        case ST_BF16 * 2: *out = OpsImpl<L, ST_BF16, false>::make(); return true;
+        case ST_BF16 * 2 + 1: *out = OpsImpl<L, ST_BF16, true>::make(); return true;
+        case ST_F64 * 2: *out = OpsImpl<L, ST_F64, false>::make(); return true;
+        case ST_F64 * 2 + 1: *out = OpsImpl<L, ST_F64, true>::make(); return true;
+        default: return false;
+    }
+}
+
+// defined in inst_<lattice>.cu
+bool ops_d2q9(int storage, int trt, Ops* out);
+bool ops_d3q15(int storage, int trt, Ops* out);
+bool ops_d3q19(int storage, int trt, Ops* out);
+bool ops_d3q27(int storage, int trt, Ops* out);
+
+}  // namespace lbm

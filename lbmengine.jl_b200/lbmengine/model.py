@@ -1,0 +1,207 @@
+"""Python mirror of LBMengine.jl's model API over the C ABI.
+
+Names, keywords, defaults and error behaviour follow the reference's exported
+API (src/LBMengine.jl:27-41); Julia's `f!` functions are spelled without the
+bang.  Arrays are numpy views in the reference's column-major layout:
+``model.massDensity[i, j, k]`` is the reference's ``massDensity[i+1, j+1, k+1]``.
+All computation happens in liblbm_b200.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _capi as capi
+from . import config as cfgmod
+from .config import DEFAULT
+
+
+class LBMparticle(SimpleNamespace):
+    """Snapshot of LBMparticle (src/gpu/structs.jl:85-95) after a tick."""
+
+
+class LBMmodel:
+    """A model living on the GPU (LBMmodel, src/gpu/structs.jl:52-76)."""
+
+    def __init__(self, resolved, lib=None):
+        self._lib = lib or capi.load()
+        self._res = resolved
+        self._h = C.c_void_p()
+        capi.check(self._lib, None, self._lib.lbm_create(C.byref(resolved.cfg), C.byref(self._h)))
+        self.schemes = list(resolved.schemes)
+        self.spaceTime = SimpleNamespace(coordinates=resolved.coordinates, latticeParameter=resolved.dt,
+                                         timeStep=resolved.dt, latticeSpeed=1.0, dims=resolved.dims)
+        self.fluidParams = SimpleNamespace(relaxationTime=resolved.tau, viscosity=resolved.viscosity,
+                                           relaxationTimePlus=resolved.tau, relaxationTimeMinus=resolved.tau_minus,
+                                           c_s=3 ** -0.5, c2_s=1 / 3, c4_s=1 / 9, invC_s=3 ** 0.5, invC2_s=3.0,
+                                           invC4_s=9.0)
+        self.particleInteractions = []
+        self._shape = resolved.shape
+        self._dims = resolved.dims
+        info = self.info()
+        self._q = info.q
+        self._cells = info.cells
+
+    # ---- handle plumbing -------------------------------------------------
+    def _check(self, code):
+        capi.check(self._lib, self._h, code)
+
+    def info(self):
+        inf = capi.LbmInfo()
+        self._check(self._lib.lbm_get_info(self._h, C.byref(inf)))
+        return inf
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            self._lib.lbm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- reference fields --------------------------------------------------
+    @property
+    def tick(self) -> int:
+        return int(self.info().tick)
+
+    @property
+    def time(self) -> float:
+        return float(self.info().time)
+
+    def _fields(self):
+        rho = np.empty(self._cells, dtype=np.float64)
+        u = np.empty(self._cells * self._dims, dtype=np.float64)
+        self._check(self._lib.lbm_get_fields(self._h, rho.ctypes.data_as(capi._dp), u.ctypes.data_as(capi._dp)))
+        return rho, u
+
+    @property
+    def massDensity(self) -> np.ndarray:
+        rho, _ = self._fields()
+        return rho.reshape(self._shape, order="F")
+
+    @property
+    def fluidVelocity(self) -> np.ndarray:
+        _, u = self._fields()
+        return u.reshape(self._shape + (self._dims,), order="F")
+
+    @property
+    def distributions(self) -> np.ndarray:
+        f = np.empty(self._cells * self._q, dtype=np.float64)
+        self._check(self._lib.lbm_get_distributions(self._h, f.ctypes.data_as(capi._dp)))
+        return f.reshape(self._shape + (self._q,), order="F")
+
+    @distributions.setter
+    def distributions(self, f):
+        f = np.asfortranarray(np.asarray(f, dtype=np.float64))
+        if f.shape != self._shape + (self._q,):
+            raise ValueError(f"distributions must have shape {self._shape + (self._q,)}")
+        flat = np.ascontiguousarray(f.ravel(order="F"))
+        self._check(self._lib.lbm_set_distributions(self._h, flat.ctypes.data_as(capi._dp)))
+
+    def particle_states(self):
+        cnt = C.c_int32()
+        self._check(self._lib.lbm_get_particles(self._h, None, 0, C.byref(cnt)))
+        if cnt.value == 0:
+            return []
+        arr = (capi.LbmParticleState * cnt.value)()
+        self._check(self._lib.lbm_get_particles(self._h, arr, cnt.value, C.byref(cnt)))
+        return list(arr)
+
+    @property
+    def particles(self):
+        d = self._dims
+        out = []
+        for s in self.particle_states():
+            props = ["spherical", "bead" if s.kind == capi.LBM_BEAD else "squirmer"]
+            pp = SimpleNamespace(radius=s.radius, inverseMass=s.inverse_mass,
+                                 inverseMomentOfInertia=s.inverse_inertia, properties=props,
+                                 coupleForces=bool(s.couple_forces), coupleTorques=bool(s.couple_torques))
+            if s.kind == capi.LBM_SQUIRMER:
+                pp.B1, pp.B2 = s.B1, s.B2
+                pp.swimmingDirection = np.array(s.swimming_direction[:d])
+            out.append(LBMparticle(
+                id=s.id, particleParams=pp,
+                position=np.array(s.position[:d]), velocity=np.array(s.velocity[:d]),
+                angularVelocity=(s.angular_velocity[0] if d == 2 else np.array(s.angular_velocity[:3])),
+                forceInput=np.zeros(d), torqueInput=(0.0 if d == 2 else np.zeros(3)),
+                lastForce=np.array(s.last_force[:d]),
+                lastTorque=(s.last_torque[0] if d == 2 else np.array(s.last_torque[:3]))))
+        return out
+
+    def solid_region(self, pid: int) -> np.ndarray:
+        m = np.empty(self._cells, dtype=np.uint8)
+        self._check(self._lib.lbm_get_mask(self._h, pid, m.ctypes.data_as(capi._u8p)))
+        return m.reshape(self._shape, order="F").astype(bool)
+
+    def boundary_links(self, pid: int):
+        n = C.c_int64()
+        self._check(self._lib.lbm_get_links(self._h, pid, None, None, 0, C.byref(n)))
+        cells = np.empty(max(1, n.value), dtype=np.int64)
+        dirs = np.empty(max(1, n.value), dtype=np.int8)
+        self._check(self._lib.lbm_get_links(self._h, pid, cells.ctypes.data_as(C.POINTER(C.c_int64)),
+                                            dirs.ctypes.data_as(C.POINTER(C.c_int8)), n.value, C.byref(n)))
+        return cells[:n.value], dirs[:n.value]
+
+    def step(self, n: int) -> None:
+        self._check(self._lib.lbm_step(self._h, int(n)))
+
+    def save_state(self, path: str) -> None:
+        self._check(self._lib.lbm_save_state(self._h, path.encode()))
+
+    def load_state(self, path: str) -> None:
+        self._check(self._lib.lbm_load_state(self._h, path.encode()))
+
+
+def modelInit(**kw) -> LBMmodel:
+    """modelInit(; ...) — src/gpu/initMethods.jl:440-702.
+
+    Extra keywords of this build: ``storage`` ("f32" default, "f16", "bf16",
+    "f64"), ``rho_ref`` and ``store_scale`` (shifted-storage parameters).
+    """
+    return LBMmodel(cfgmod.resolve_model(**kw))
+
+
+def _add(model: LBMmodel, params) -> int:
+    pid = C.c_int32()
+    model._check(model._lib.lbm_add_particle(model._h, C.byref(params), C.byref(pid)))
+    for s in ("ladd", "bounceBack"):
+        if s not in model.schemes:
+            model.schemes.append(s)
+    return pid.value
+
+
+def addSquirmer(model: LBMmodel, **kw) -> None:
+    """addSquirmer!(model; ...) — src/gpu/initMethods.jl:91-222."""
+    _add(model, cfgmod.resolve_squirmer(model._dims, **kw))
+
+
+def addBead(model: LBMmodel, **kw) -> None:
+    """addBead!(model; ...) — src/gpu/initMethods.jl:7-89."""
+    _add(model, cfgmod.resolve_bead(model._dims, **kw))
+
+
+def LBMpropagate(model: LBMmodel, simulationTime=DEFAULT, ticks=DEFAULT, verbose=False, ticksSaved=DEFAULT) -> None:
+    """LBMpropagate!(model; simulationTime, ticks, verbose, ticksSaved) — src/gpu/fluids.jl:228-264."""
+    n = cfgmod.propagate_ticks(model.spaceTime.timeStep, simulationTime, ticks)
+    model.step(n)
+    if verbose:
+        print(f"\r t = {round(model.time, 2)}")
+
+
+def hydroVariablesUpdate(model: LBMmodel, useEquilibriumScheme=False) -> None:
+    """hydroVariablesUpdate! — src/gpu/fluids.jl:32-37.
+
+    The library keeps rho and u consistent with the populations at all times
+    (they are evaluated from model.distributions on read), so this is a no-op
+    kept for API compatibility.
+    """
+    return None

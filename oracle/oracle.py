@@ -1,0 +1,164 @@
+"""ctypes driver of the FP64 CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg,
+always as the checker or the timed CPU baseline, never as a product path.
+The oracle restates LBMengine.jl's GPU-module time step in FP64; parity is
+unpinned by the reference itself (it ships no tests or golden vectors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+PKG = os.path.join(REPO, "lbmengine.jl_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+
+from lbmengine import _capi as capi  # noqa: E402  (struct layouts of include/lbm_b200.h)
+
+LIB_PATH = os.path.join(HERE, "_build", "liblbm_oracle.so")
+
+_lib = None
+
+
+def build(quiet: bool = True) -> str:
+    """Compile the oracle with its Makefile (g++, OpenMP, no FP contraction)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    lib.orc_last_error.restype = C.c_char_p
+    lib.orc_set_threads.argtypes = [C.c_int]
+    lib.orc_max_threads.restype = C.c_int
+    lib.orc_create.argtypes = [C.POINTER(capi.LbmConfig), C.POINTER(vp)]
+    lib.orc_add_particle.argtypes = [vp, C.POINTER(capi.LbmParticleParams), C.POINTER(C.c_int32)]
+    lib.orc_step.argtypes = [vp, C.c_int64]
+    lib.orc_get_fields.argtypes = [vp, dp, dp]
+    lib.orc_get_distributions.argtypes = [vp, dp]
+    lib.orc_set_distributions.argtypes = [vp, dp]
+    lib.orc_get_particles.argtypes = [vp, C.POINTER(capi.LbmParticleState), C.c_int32, C.POINTER(C.c_int32)]
+    lib.orc_get_mask.argtypes = [vp, C.c_int32, C.POINTER(C.c_uint8)]
+    lib.orc_get_links.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.c_int64,
+                                  C.POINTER(C.c_int64)]
+    lib.orc_get_info.argtypes = [vp, C.POINTER(capi.LbmInfo)]
+    lib.orc_velocity_set.argtypes = [C.c_int32, C.POINTER(C.c_int8), dp, C.POINTER(C.c_int32)]
+    lib.orc_destroy.argtypes = [vp]
+    _lib = lib
+    return lib
+
+
+def _check(code):
+    if code != 0:
+        raise capi.LbmError(code, load().orc_last_error().decode())
+
+
+def velocity_set(q: int):
+    lib = load()
+    c = np.zeros((q, 3), dtype=np.int8)
+    w = np.zeros(q, dtype=np.float64)
+    opp = np.zeros(q, dtype=np.int32)
+    _check(lib.orc_velocity_set(q, c.ctypes.data_as(C.POINTER(C.c_int8)), w.ctypes.data_as(C.POINTER(C.c_double)),
+                                opp.ctypes.data_as(C.POINTER(C.c_int32))))
+    return c, w, opp
+
+
+def set_threads(n: int) -> None:
+    load().orc_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(load().orc_max_threads())
+
+
+class OracleModel:
+    """One FP64 CPU model built from a resolved config (lbmengine.config.resolve_model)."""
+
+    def __init__(self, resolved):
+        self.lib = load()
+        self.res = resolved
+        self.h = C.c_void_p()
+        _check(self.lib.orc_create(C.byref(resolved.cfg), C.byref(self.h)))
+        info = self.info()
+        self.q = info.q
+        self.dims = info.dims
+        self.shape = tuple(info.n[a] for a in range(self.dims))
+        self.cells = info.cells
+
+    def info(self):
+        inf = capi.LbmInfo()
+        _check(self.lib.orc_get_info(self.h, C.byref(inf)))
+        return inf
+
+    def add_particle(self, params) -> int:
+        pid = C.c_int32()
+        _check(self.lib.orc_add_particle(self.h, C.byref(params), C.byref(pid)))
+        return pid.value
+
+    def step(self, n: int) -> None:
+        _check(self.lib.orc_step(self.h, int(n)))
+
+    def fields(self):
+        rho = np.zeros(self.cells, dtype=np.float64)
+        u = np.zeros(self.cells * self.dims, dtype=np.float64)
+        _check(self.lib.orc_get_fields(self.h, rho.ctypes.data_as(capi._dp), u.ctypes.data_as(capi._dp)))
+        return rho, u.reshape(self.dims, self.cells)
+
+    def distributions(self):
+        f = np.zeros(self.cells * self.q, dtype=np.float64)
+        _check(self.lib.orc_get_distributions(self.h, f.ctypes.data_as(capi._dp)))
+        return f.reshape(self.q, self.cells)
+
+    def set_distributions(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).ravel()
+        _check(self.lib.orc_set_distributions(self.h, f.ctypes.data_as(capi._dp)))
+
+    def particles(self):
+        cnt = C.c_int32()
+        _check(self.lib.orc_get_particles(self.h, None, 0, C.byref(cnt)))
+        arr = (capi.LbmParticleState * max(1, cnt.value))()
+        _check(self.lib.orc_get_particles(self.h, arr, cnt.value, C.byref(cnt)))
+        return list(arr)[:cnt.value]
+
+    def mask(self, pid: int):
+        m = np.zeros(self.cells, dtype=np.uint8)
+        _check(self.lib.orc_get_mask(self.h, pid, m.ctypes.data_as(capi._u8p)))
+        return m
+
+    def links(self, pid: int):
+        n = C.c_int64()
+        _check(self.lib.orc_get_links(self.h, pid, None, None, 0, C.byref(n)))
+        cells = np.zeros(max(1, n.value), dtype=np.int64)
+        dirs = np.zeros(max(1, n.value), dtype=np.int8)
+        _check(self.lib.orc_get_links(self.h, pid, cells.ctypes.data_as(C.POINTER(C.c_int64)),
+                                      dirs.ctypes.data_as(C.POINTER(C.c_int8)), n.value, C.byref(n)))
+        return cells[:n.value], dirs[:n.value]
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,109 @@
+"""GPU parity: liblbm_b200.so (through the C ABI) against the FP64 CPU oracle.
+
+Tolerances (stated per storage format):
+  * masks and boundary-link lists: bit-exact;
+  * FP64 storage: fields and particle state within 1e-10 (relative L2 / absolute);
+  * FP32 storage (shifted populations, FP32 collision): density and velocity
+    relative L2 <= 1e-5, particle position within 1e-7 lattice units.
+"""
+from __future__ import annotations
+
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from parity_cases import CASES, build_pair, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": dict(field=1e-10, pos=1e-10, vel=1e-10, force=1e-8),
+       "f32": dict(field=1e-5, pos=1e-7, vel=1e-7, force=5e-4)}
+
+
+def _compare(res, gpu, orc, storage, tag):
+    tol = TOL[storage]
+    rho_o, u_o = orc.fields()
+    rho_g = gpu.massDensity.ravel(order="F")
+    u_g = gpu.fluidVelocity.reshape(-1, res.dims, order="F").T
+    assert rel_l2(rho_g, rho_o) <= tol["field"], f"{tag}: rho rel L2 {rel_l2(rho_g, rho_o):.3e}"
+    du = rel_l2(u_g, u_o)
+    assert du <= tol["field"] * (10 if storage == "f32" else 1), f"{tag}: u rel L2 {du:.3e}"
+    pg, po = gpu.particle_states(), orc.particles()
+    assert len(pg) == len(po)
+    d = res.dims
+    for a, b in zip(pg, po):
+        assert np.max(np.abs(np.array(a.position[:d]) - np.array(b.position[:d]))) <= tol["pos"], tag
+        vscale = max(1e-6, np.max(np.abs(b.velocity[:d])))
+        assert np.max(np.abs(np.array(a.velocity[:d]) - np.array(b.velocity[:d]))) <= tol["vel"] * max(1.0, vscale * 1e3), tag
+        np.testing.assert_allclose(a.swimming_direction[:d], b.swimming_direction[:d], atol=1e-9, rtol=0)
+        fscale = max(1e-12, np.max(np.abs(b.last_force[:d])))
+        assert np.max(np.abs(np.array(a.last_force[:d]) - np.array(b.last_force[:d]))) <= tol["force"] * fscale + 1e-14, \
+            f"{tag}: force {list(a.last_force[:d])} vs {list(b.last_force[:d])}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_parity_fields_and_trajectories(lib, oracle_mod, name, storage):
+    case = CASES[name]
+    res, gpu, orc = build_pair(case, storage=storage, oracle_mod=oracle_mod)
+    _compare(res, gpu, orc, storage, f"{name}/{storage}/t0")
+    steps = case["steps"]
+    for chunk in (1, steps // 2 - 1, steps - steps // 2):
+        gpu.step(chunk)
+        orc.step(chunk)
+    assert gpu.tick == orc.info().tick == steps
+    _compare(res, gpu, orc, storage, f"{name}/{storage}/t{steps}")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_masks_and_links_bit_exact(lib, oracle_mod, name):
+    case = CASES[name]
+    if not case["particles"]:
+        pytest.skip("no particles")
+    res, gpu, orc = build_pair(case, storage="f64", oracle_mod=oracle_mod)
+    for pid in range(1, len(case["particles"]) + 1):
+        np.testing.assert_array_equal(gpu.solid_region(pid).ravel(order="F").astype(np.uint8), orc.mask(pid))
+        cg, dg = gpu.boundary_links(pid)
+        co, do = orc.links(pid)
+        np.testing.assert_array_equal(cg, co)
+        np.testing.assert_array_equal(dg, do)
+    gpu.step(case["steps"])
+    orc.step(case["steps"])
+    for pid, (a, b) in enumerate(zip(gpu.particle_states(), orc.particles()), start=1):
+        if tuple(a.position) == tuple(b.position):
+            np.testing.assert_array_equal(gpu.solid_region(pid).ravel(order="F").astype(np.uint8), orc.mask(pid))
+
+
+def test_distributions_roundtrip_and_checkpoint(lib, oracle_mod):
+    case = CASES["d3q19_multi"]
+    res, gpu, _ = build_pair(case, storage="f32")
+    gpu.step(7)
+    f = gpu.distributions
+    rho = gpu.massDensity
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "state.lbm")
+        gpu.save_state(path)
+        gpu.step(5)
+        ref_after = gpu.fluidVelocity.copy()
+        pos_after = [tuple(p.position) for p in gpu.particle_states()]
+        gpu.load_state(path)
+        assert gpu.tick == 7
+        np.testing.assert_array_equal(gpu.massDensity, rho)
+        gpu.step(5)
+        np.testing.assert_array_equal(gpu.fluidVelocity, ref_after)
+        assert [tuple(p.position) for p in gpu.particle_states()] == pos_after
+    gpu.distributions = f
+    np.testing.assert_allclose(gpu.distributions, f, rtol=0, atol=1e-7)
+
+
+def test_mass_conservation_periodic(lib):
+    from lbmengine import modelInit
+    rng = np.random.default_rng(3)
+    m = modelInit(dims=3, velocities="D3Q19", collisionModel="trt", latticeParameter=1.0, relaxationTimeRatio=0.6,
+                  xlims=(0.0, 31.0), massDensity=1.0 + 1e-3 * rng.standard_normal((32, 32, 32)),
+                  fluidVelocity=np.zeros((32, 32, 32, 3)), storage="f32")
+    m0 = m.massDensity.sum()
+    m.step(200)
+    assert abs(m.massDensity.sum() - m0) / m0 < 1e-6
