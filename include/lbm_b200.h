@@ -209,17 +209,29 @@ int lbm_get_info(lbm_handle* h, lbm_info* info);
 typedef struct lbm_profile {
     double total_ms;        /* device time of the whole lbm_step call */
     double bulk_ms;         /* mean duration of one bulk stream-collide launch */
-    double boundary_ms;     /* mean duration of one boundary-tile launch (0 if none) */
+    double fixup_ms;        /* mean duration of one boundary-link fix-up launch (0 if none) */
     double particles_ms;    /* mean duration of one particle-update launch (0 if none) */
     int64_t steps;          /* ticks in the call */
     int64_t launches;       /* kernel launches enqueued by the call */
     int64_t profiled_steps; /* ticks whose kernels were bracketed by events */
-    int64_t bulk_cells;     /* lattice nodes updated by the bulk kernel in the last tick */
-    int64_t boundary_tiles; /* tiles handled by the boundary kernel in the last tick */
+    int64_t bulk_cells;     /* lattice nodes updated by the bulk kernel per tick */
+    int64_t fixup_entries;  /* nodes the boundary fix-up examines per tick (particle near boxes + wall-link nodes) */
 } lbm_profile;
 
-int lbm_set_profiling(lbm_handle* h, int32_t on);
+/* level 0: off; 1: device time of each lbm_step call; 2: also per-kernel
+ * durations (event nodes around every kernel of the step graph) */
+int lbm_set_profiling(lbm_handle* h, int32_t level);
 int lbm_get_profile(lbm_handle* h, lbm_profile* out);
+
+/* Mean device duration of one launch of a single kernel of the tick
+ * (0: bulk stream-collide, 1: boundary-link fix-up, 2: particle update),
+ * from CUDA events around `launches` back-to-back launches on the handle's
+ * stream.  The model state is saved before and restored after, so the
+ * simulation is unaffected.  No counterpart in the reference. */
+#define LBM_KERNEL_BULK 0
+#define LBM_KERNEL_FIXUP 1
+#define LBM_KERNEL_PARTICLES 2
+int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg_ms);
 
 /* Raw checkpoint of populations + particle FP64 state + tick/time. */
 int lbm_save_state(lbm_handle* h, const char* path);

@@ -147,14 +147,14 @@ __global__ void k_init(const InitArgs a) {
 
 struct MaskArgs {
     unsigned char* mask;
-    const double* coord[3];
+    const ParticleDev* part;
+    const int2* ivl;
     int n[3];
     long long N;
-    double c[3];
-    double r2;
 };
 
-// getSphere over the whole grid (src/gpu/aux.jl:206-215)
+// solidRegion of one particle over the whole grid (getSphere, src/gpu/aux.jl:206-215),
+// read from the row intervals that the fix-up kernel uses
 template <int D>
 __global__ void k_mask(const MaskArgs a) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -162,7 +162,7 @@ __global__ void k_mask(const MaskArgs a) {
     const int x = (int)(q % a.n[0]);
     const int y = (int)((q / a.n[0]) % a.n[1]);
     const int z = (int)(q / ((long long)a.n[0] * a.n[1]));
-    a.mask[q] = sphere_test<D>(a.coord[0][x], a.coord[1][y], D == 3 ? a.coord[2][z] : 0.0, a.c, a.r2) ? 1 : 0;
+    a.mask[q] = solid_at(*a.part, a.ivl, x, y, z) ? 1 : 0;
 }
 
 // device-side scan for non-finite or non-positive densities (fault detection)

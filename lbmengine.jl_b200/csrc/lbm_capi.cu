@@ -2,8 +2,9 @@
 //
 // Host side of the drop-in boundary: validates the resolved modelInit /
 // addSquirmer! keyword sets, owns all device memory of a model, and runs
-// LBMpropagate! as CUDA-graph replays of the fused tick
-// (k_boundary || k_bulk) -> k_particles on one stream.
+// LBMpropagate! as CUDA-graph replays of the tick
+//     k_bulk(_v4) -> k_fixup -> k_particles
+// on one stream.
 #include "lbm_b200.h"
 #include "ops.cuh"
 
@@ -21,13 +22,14 @@ namespace {
 thread_local std::string g_global_err;
 
 const char* kBuildInfo =
-    "lbm_b200: sm_100a fused push collide-stream (BGK/TRT + Guo), halfway bounce-back, "
-    "Ladd squirmer coupling; storage f32/f16/bf16/f64";
+    "lbm_b200: sm_100a vectorised push collide-stream (BGK/TRT + Guo), boundary-link fix-up "
+    "(halfway bounce-back, moving walls, Ladd squirmers); storage f32/f16/bf16/f64";
 
 struct Graph {
     cudaGraphExec_t exec = nullptr;
-    int start_buf = -1;
 };
+
+constexpr int kGraphSteps = 16;
 
 }  // namespace
 
@@ -44,29 +46,34 @@ struct lbm_handle {
     double F[3] = {0, 0, 0};
     int incompressible = 0;
     double rho_inc = 1;
-    bool has_walls = false, moving_walls = false;
+    bool has_walls = false;
     std::vector<double> X[3];
     Ops ops{};
-    // device state
+    // device state: the main stream and a side stream for the particle update
     cudaStream_t stream = nullptr, side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fix = nullptr, ev_part = nullptr;
+    bool part_pending = false;
     void* pop[2] = {nullptr, nullptr};
     int cur = 0;
     double* d_coord[3] = {nullptr, nullptr, nullptr};
     unsigned char* d_wall = nullptr;
     double* d_uw = nullptr;
     double* d_ffield = nullptr;
-    unsigned char* d_tileflags = nullptr;
-    int* d_walltiles = nullptr;
-    int nwalltiles = 0;
+    int2* d_wlinks = nullptr;   // static wall-link entries (cell, mask)
+    int* d_wnodes = nullptr;    // static wall nodes
+    int nwlinks = 0, nwnodes = 0;
     unsigned long long* d_tilebits = nullptr;
     int words = 1;
     ParticleDev* d_parts = nullptr;
     int pcap = 0;
-    std::vector<ParticleDev> hparts;  // host copy of the static fields
+    std::vector<ParticleDev> hparts;  // host copy of the static fields (offsets, capacities)
+    int2* d_ivl = nullptr;
+    long long ivl_slots = 0;
+    int2* d_links = nullptr;
+    long long link_slots = 0;
     double* d_partial = nullptr;
     long long partial_slots = 0;
-    int maxtl = 0;
+    int maxchunks = 0;
     int* d_err = nullptr;
     double* d_tmp = nullptr;  // FP64 read-back / upload scratch
     size_t tmp_bytes = 0;
@@ -74,11 +81,11 @@ struct lbm_handle {
     // time
     long long tick = 0;
     double time = 0;
-    // graphs of kGraphSteps ticks, one per starting buffer; [1] with event nodes
+    // graphs of kGraphSteps ticks: [profiling][starting buffer]
     Graph graphs[2][2];
-    // profiling: per graph slot, events before/after the bulk kernel, around the
-    // boundary kernel and after the particle kernel; plus the whole call
-    bool profiling = false;
+    // profiling: per graph slot, events before/after the bulk kernel, after
+    // the fix-up and after the particle kernel; plus the whole call
+    int profiling = 0;  // 0 off, 1 whole-call time, 2 also per-kernel event nodes
     std::vector<cudaEvent_t> pev;
     cudaEvent_t t_begin = nullptr, t_end = nullptr;
     lbm_profile prof{};
@@ -86,8 +93,6 @@ struct lbm_handle {
 };
 
 namespace {
-
-constexpr int kGraphSteps = 16;
 
 int set_err(lbm_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
@@ -142,7 +147,7 @@ bool get_ops(int lattice, int storage, int trt, Ops* o) {
     }
 }
 
-// host copy of the lattice (for link enumeration and checks)
+// host copy of the lattice (link enumeration, Guo constants)
 struct HostLattice {
     int q = 0, d = 0;
     std::vector<int> cx, cy, cz, opp;
@@ -173,6 +178,15 @@ HostLattice host_lattice(int lattice) {
     }
 }
 
+int storage_bytes(int storage) {
+    switch (storage) {
+        case LBM_STORE_F16:
+        case LBM_STORE_BF16: return 2;
+        case LBM_STORE_F64: return 8;
+        default: return 4;
+    }
+}
+
 int ensure_tmp(lbm_handle* h, size_t bytes) {
     if (h->tmp_bytes >= bytes) return LBM_OK;
     dev_free(h->d_tmp);
@@ -189,7 +203,6 @@ void drop_graphs(lbm_handle* h) {
         for (auto& gr : row) {
             if (gr.exec) cudaGraphExecDestroy(gr.exec);
             gr.exec = nullptr;
-            gr.start_buf = -1;
         }
 }
 
@@ -200,16 +213,19 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.g = h->g;
     for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
     a.tilebits = h->d_tilebits;
-    a.tileflags = h->d_tileflags;
-    a.walltiles = h->d_walltiles;
-    a.nwalltiles = h->nwalltiles;
     a.words = h->words;
+    a.nparts = (int)h->hparts.size();
     a.wall = h->d_wall;
     a.uw = h->d_uw;
     a.ffield = h->d_ffield;
     a.parts = h->d_parts;
-    a.nparts = (int)h->hparts.size();
-    a.maxtl = h->maxtl;
+    a.ivl = h->d_ivl;
+    a.links = h->d_links;
+    a.wlinks = h->d_wlinks;
+    a.wnodes = h->d_wnodes;
+    a.nwlinks = h->nwlinks;
+    a.nwnodes = h->nwnodes;
+    a.maxchunks = h->maxchunks;
     a.partial = h->d_partial;
     a.err = h->d_err;
     a.rho0 = h->rho0;
@@ -227,7 +243,32 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.force_mode = h->force_mode;
     a.incompressible = h->incompressible;
     a.rho_inc = h->rho_inc;
+    // Guo constants (collide(): BGK A_i + K0 + B_i cu ; TRT even K0 + B_i cu, odd A_i)
+    const double kodd = h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k;
+    const double keven = h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k;
+    a.gK0 = h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k;
+    a.gkA = kodd;
+    a.gkB = keven;
+    const HostLattice hl = host_lattice(h->lattice);
+    const size_t esz = storage_bytes(h->storage);
+    for (int i = 0; i < 27; ++i) {
+        a.gA[i] = a.gB[i] = 0.0;
+        a.srcq[i] = nullptr;
+        a.dstq[i] = nullptr;
+    }
+    for (int i = 0; i < hl.q; ++i) {
+        const double cF = hl.cx[i] * h->F[0] + hl.cy[i] * h->F[1] + hl.cz[i] * h->F[2];
+        a.gA[i] = kodd * cF;
+        a.gB[i] = keven * cF;
+        a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
+        a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
+    }
     return a;
+}
+
+bool use_vector_bulk(const lbm_handle* h) {
+    return h->ops.bulk_v4 != nullptr && h->force_mode != LBM_FORCE_FIELD && h->n[0] % 4 == 0 &&
+           h->g.t[0] == h->n[0] && (h->n[0] / 4) * h->g.t[1] <= kBlockV4;
 }
 
 ParticleArgs particle_args(const lbm_handle* h, int mode, int pid) {
@@ -236,9 +277,11 @@ ParticleArgs particle_args(const lbm_handle* h, int mode, int pid) {
     a.nparts = (int)h->hparts.size();
     a.mode = mode;
     a.setup_pid = pid;
+    a.words = h->words;
     a.partial = h->d_partial;
     a.tilebits = h->d_tilebits;
-    a.words = h->words;
+    a.ivl = h->d_ivl;
+    a.links = h->d_links;
     a.g = h->g;
     for (int k = 0; k < 3; ++k) {
         a.coord[k] = h->d_coord[k];
@@ -265,43 +308,70 @@ CodecArgs codec_args(const lbm_handle* h) {
     return c;
 }
 
-// events of graph slot s: [0] before bulk, [1] after bulk, [2] before boundary,
-// [3] after boundary, [4] after particles
-cudaEvent_t prof_event(lbm_handle* h, int slot, int k) { return h->pev[slot * 5 + k]; }
-
-void prof_record(lbm_handle* h, int slot, int k, cudaStream_t s) {
-    if (h->profiling) cudaEventRecordWithFlags(prof_event(h, slot, k), s, cudaEventRecordExternal);
-}
-
-// enqueue one tick on h->stream (capturable); `slot` selects the profiling events
-void enqueue_tick(lbm_handle* h, int src, int slot) {
-    const StepArgs a = step_args(h, src);
-    const dim3 block(h->g.t[0], h->g.t[1], h->g.t[2]);
-    const long long nb = (long long)a.nparts * a.maxtl + a.nwalltiles;
-    if (nb > 0) {
-        // boundary tiles on a side branch, concurrent with the bulk tiles
-        cudaEventRecord(h->ev_fork, h->stream);
-        cudaStreamWaitEvent(h->side, h->ev_fork, 0);
-        prof_record(h, slot, 2, h->side);
-        h->ops.boundary(a, (unsigned)nb, block, h->side);
-        prof_record(h, slot, 3, h->side);
-        cudaEventRecord(h->ev_join, h->side);
-    }
-    prof_record(h, slot, 0, h->stream);
-    h->ops.bulk(a, (unsigned)h->g.ntiles, block, h->stream);
-    prof_record(h, slot, 1, h->stream);
-    if (nb > 0) cudaStreamWaitEvent(h->stream, h->ev_join, 0);
-    if (a.nparts > 0) h->ops.particles(particle_args(h, 0, 0), (unsigned)a.nparts, h->stream);
-    prof_record(h, slot, 4, h->stream);
+long long fixup_blocks(const lbm_handle* h) {
+    return (long long)h->hparts.size() * h->maxchunks + (h->nwlinks + kFixBlock - 1) / kFixBlock +
+           (h->nwnodes + kFixBlock - 1) / kFixBlock;
 }
 
 int launches_per_tick(const lbm_handle* h) {
-    const long long nb = (long long)h->hparts.size() * h->maxtl + h->nwalltiles;
-    return 1 + (nb > 0 ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
+    return 1 + (fixup_blocks(h) > 0 ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
+}
+
+// events of graph slot s: [0] before bulk, [1] after bulk, [2] after fix-up, [3] after particles
+cudaEvent_t prof_event(lbm_handle* h, int slot, int k) { return h->pev[slot * 4 + k]; }
+
+void prof_record(lbm_handle* h, int slot, int k, cudaStream_t s) {
+    if (h->profiling < 2) return;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &st);
+    // inside a capture the record becomes an event node of the graph
+    if (st == cudaStreamCaptureStatusActive)
+        cudaEventRecordWithFlags(prof_event(h, slot, k), s, cudaEventRecordExternal);
+    else
+        cudaEventRecord(prof_event(h, slot, k), s);
+}
+
+// Enqueue one tick (capturable); `slot` selects the profiling events.
+// Stream order:  main: bulk(n) -> [wait particles(n-1)] -> fixup(n) -> bulk(n+1) ...
+//                side:                    particles(n) after fixup(n)
+// The bulk pass never reads particle state, so the particle update of tick n
+// runs concurrently with the bulk pass of tick n+1.
+void enqueue_tick(lbm_handle* h, int src, int slot) {
+    const StepArgs a = step_args(h, src);
+    prof_record(h, slot, 0, h->stream);
+    if (use_vector_bulk(h))
+        h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
+    else
+        h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+    prof_record(h, slot, 1, h->stream);
+    if (h->part_pending) {
+        cudaStreamWaitEvent(h->stream, h->ev_part, 0);
+        h->part_pending = false;
+    }
+    const long long nb = fixup_blocks(h);
+    if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
+    if (a.nparts == 0) prof_record(h, slot, 2, h->stream);
+    if (a.nparts > 0) {
+        cudaEventRecord(h->ev_fix, h->stream);
+        cudaStreamWaitEvent(h->side, h->ev_fix, 0);
+        prof_record(h, slot, 2, h->side);
+        h->ops.particles(particle_args(h, 0, 0), (unsigned)a.nparts, h->side);
+        prof_record(h, slot, 3, h->side);
+        cudaEventRecord(h->ev_part, h->side);
+        h->part_pending = true;
+    }
+}
+
+// make the main stream wait for an outstanding particle update
+void join_particles(lbm_handle* h) {
+    if (h->part_pending) {
+        cudaStreamWaitEvent(h->stream, h->ev_part, 0);
+        h->part_pending = false;
+    }
 }
 
 int build_graph(lbm_handle* h, int start) {
-    Graph& gr = h->graphs[h->profiling ? 1 : 0][start];
+    Graph& gr = h->graphs[h->profiling >= 2 ? 1 : 0][start];
     if (gr.exec) return LBM_OK;
     cudaGraph_t graph = nullptr;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -310,6 +380,7 @@ int build_graph(lbm_handle* h, int start) {
         enqueue_tick(h, b, s);
         b = 1 - b;
     }
+    join_particles(h);  // a capture must end with every forked stream joined
     cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -321,7 +392,6 @@ int build_graph(lbm_handle* h, int start) {
         gr.exec = nullptr;
         return set_err(h, LBM_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
     }
-    gr.start_buf = start;
     return LBM_OK;
 }
 
@@ -329,19 +399,17 @@ int check_device_error(lbm_handle* h) {
     int err = 0;
     CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    if (err & kErrTooManyCandidates)
-        return set_err(h, LBM_ERR_UNSUPPORTED, "more than 16 particles meet one tile of the lattice");
-    if (err & kErrPartialOverflow) return set_err(h, LBM_ERR_STATE, "particle tile box exceeded its partial-sum capacity");
+    if (err & kErrLinkOverflow) return set_err(h, LBM_ERR_STATE, "particle boundary links exceeded their capacity");
+    if (err & kErrIntervalOverflow) return set_err(h, LBM_ERR_STATE, "particle solid box exceeded its capacity");
     return LBM_OK;
 }
 
-// choose the CTA tile: full x-rows up to 256 nodes (x-wrap stays inside the CTA)
+// CTA tile: full x-rows up to 256 nodes (x-wrap stays inside the CTA)
 void choose_tiles(lbm_handle* h) {
     GridDesc& g = h->g;
     for (int k = 0; k < 3; ++k) g.n[k] = h->n[k];
-    int t0 = std::min(256, ((h->n[0] + 31) / 32) * 32);
-    int t1 = std::max(1, std::min(256 / t0, h->n[1]));
-    // keep the CTA a multiple of 32 threads
+    const int t0 = std::min(256, ((h->n[0] + 31) / 32) * 32);
+    const int t1 = std::max(1, std::min(256 / t0, h->n[1]));
     g.t[0] = t0;
     g.t[1] = t1;
     g.t[2] = 1;
@@ -366,73 +434,75 @@ void destroy_all(lbm_handle* h) {
     dev_free(h->d_wall);
     dev_free(h->d_uw);
     dev_free(h->d_ffield);
-    dev_free(h->d_tileflags);
-    dev_free(h->d_walltiles);
+    dev_free(h->d_wlinks);
+    dev_free(h->d_wnodes);
     dev_free(h->d_tilebits);
     dev_free(h->d_parts);
+    dev_free(h->d_ivl);
+    dev_free(h->d_links);
     dev_free(h->d_partial);
     dev_free(h->d_err);
     dev_free(h->d_tmp);
     for (auto& e : h->pev) cudaEventDestroy(e);
     if (h->t_begin) cudaEventDestroy(h->t_begin);
     if (h->t_end) cudaEventDestroy(h->t_end);
-    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_fix) cudaEventDestroy(h->ev_fix);
+    if (h->ev_part) cudaEventDestroy(h->ev_part);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
 
-int storage_bytes(int storage) {
-    switch (storage) {
-        case LBM_STORE_F16:
-        case LBM_STORE_BF16: return 2;
-        case LBM_STORE_F64: return 8;
-        default: return 4;
-    }
+// grow a device array, keeping its first `keep` elements
+template <class T>
+int grow(lbm_handle* h, T** arr, long long* cap, long long need, long long keep) {
+    if (need <= *cap && *arr) return LBM_OK;
+    long long ncap = std::max<long long>(need, *cap * 2);
+    T* na = nullptr;
+    int rc = dev_alloc(h, &na, sizeof(T) * std::max<long long>(1, ncap));
+    if (rc) return rc;
+    CUDA_TRY(h, cudaMemsetAsync(na, 0, sizeof(T) * std::max<long long>(1, ncap), h->stream));
+    if (*arr && keep > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(na, *arr, sizeof(T) * keep, cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    dev_free(*arr);
+    *arr = na;
+    *cap = ncap;
+    return LBM_OK;
 }
 
-// grow device particle storage / tile-bit words / partial-sum slots
-int ensure_particle_capacity(lbm_handle* h, int nparts_new, long long slots_new) {
-    if (nparts_new > h->pcap) {
+// grow device particle storage / tile-bit words
+int ensure_particle_capacity(lbm_handle* h, int nparts_new) {
+    if (nparts_new > h->pcap || !h->d_parts) {
         int cap = std::max(8, h->pcap * 2);
         while (cap < nparts_new) cap *= 2;
         ParticleDev* np = nullptr;
         int rc = dev_alloc(h, &np, sizeof(ParticleDev) * cap);
         if (rc) return rc;
-        if (h->d_parts) {
+        if (h->d_parts && !h->hparts.empty())
             CUDA_TRY(h, cudaMemcpyAsync(np, h->d_parts, sizeof(ParticleDev) * h->hparts.size(),
                                         cudaMemcpyDeviceToDevice, h->stream));
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            dev_free(h->d_parts);
-        }
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        dev_free(h->d_parts);
         h->d_parts = np;
         h->pcap = cap;
     }
-    int words_new = (nparts_new + 63) / 64;
+    const int words_new = std::max(1, (nparts_new + 63) / 64);
     if (words_new > h->words || !h->d_tilebits) {
-        int w = std::max(words_new, h->words);
+        const int w = std::max(words_new, h->words);
         unsigned long long* nb = nullptr;
         int rc = dev_alloc(h, &nb, sizeof(unsigned long long) * h->g.ntiles * w);
         if (rc) return rc;
         CUDA_TRY(h, cudaMemsetAsync(nb, 0, sizeof(unsigned long long) * h->g.ntiles * w, h->stream));
-        if (h->d_tilebits) {
+        if (h->d_tilebits)
             CUDA_TRY(h, cudaMemcpy2DAsync(nb, sizeof(unsigned long long) * w, h->d_tilebits,
                                           sizeof(unsigned long long) * h->words,
                                           sizeof(unsigned long long) * h->words, h->g.ntiles,
                                           cudaMemcpyDeviceToDevice, h->stream));
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            dev_free(h->d_tilebits);
-        }
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        dev_free(h->d_tilebits);
         h->d_tilebits = nb;
         h->words = w;
-    }
-    if (slots_new > h->partial_slots) {
-        dev_free(h->d_partial);
-        int rc = dev_alloc(h, &h->d_partial, sizeof(double) * kPartialStride * slots_new);
-        if (rc) return rc;
-        CUDA_TRY(h, cudaMemsetAsync(h->d_partial, 0, sizeof(double) * kPartialStride * slots_new, h->stream));
-        h->partial_slots = slots_new;
     }
     return LBM_OK;
 }
@@ -443,6 +513,28 @@ bool is_uniform_axis(const std::vector<double>& X, double dx) {
         if (std::fabs(X[i] - expect) > 1e-9 * (std::fabs(expect) + std::fabs(dx) + 1.0)) return false;
     }
     return true;
+}
+
+// static wall lists: wall nodes, and fluid nodes with a wall source in some direction
+void wall_lists(const lbm_handle* h, const std::vector<unsigned char>& W, std::vector<int2>& wl,
+                std::vector<int>& wn) {
+    const HostLattice hl = host_lattice(h->lattice);
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const int c = x + nx * (y + ny * z);
+                if (W[c]) {
+                    wn.push_back(c);
+                    continue;
+                }
+                unsigned mask = 0;
+                for (int i = 1; i < hl.q; ++i) {
+                    const int tx = (x + hl.cx[i] + nx) % nx, ty = (y + hl.cy[i] + ny) % ny, tz = (z + hl.cz[i] + nz) % nz;
+                    if (W[tx + nx * (ty + ny * tz)]) mask |= 1u << hl.opp[i];  // link (x, j), x - c_j = x + c_i
+                }
+                if (mask) wl.push_back(make_int2(c, (int)mask));
+            }
 }
 
 }  // namespace
@@ -552,9 +644,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
             ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
     TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) == cudaSuccess
             ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
-    TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess
-            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "event creation failed"));
-    TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) == cudaSuccess
+    TRY(cudaEventCreateWithFlags(&h->ev_fix, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&h->ev_part, cudaEventDisableTiming) == cudaSuccess
             ? LBM_OK : set_err(h, LBM_ERR_CUDA, "event creation failed"));
     const size_t pop_bytes = (size_t)N * h->q * storage_bytes(h->storage);
     TRY(dev_alloc(h, &h->pop[0], pop_bytes));
@@ -564,7 +655,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         TRY(upload(h, h->d_coord[a], h->X[a].data(), sizeof(double) * h->n[a]));
     }
     TRY(dev_alloc(h, &h->d_err, sizeof(int)));
-    CUDA_TRY(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+    if (cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream) != cudaSuccess)
+        TRY(set_err(h, LBM_ERR_CUDA, "memset failed"));
 
     // walls (initMethods.jl:568-628): mask | {|u_w| > 0}
     std::vector<unsigned char> W;
@@ -576,54 +668,35 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
             for (long long c = 0; c < N; ++c)
                 for (int k = 0; k < h->dims; ++k)
                     if (cfg->wall_velocity[k * N + c] != 0.0) W[c] = 1;
-            h->moving_walls = true;
             TRY(dev_alloc(h, &h->d_uw, sizeof(double) * N * h->dims));
             TRY(upload(h, h->d_uw, cfg->wall_velocity, sizeof(double) * N * h->dims));
         }
         h->has_walls = true;
         TRY(dev_alloc(h, &h->d_wall, N));
         TRY(upload(h, h->d_wall, W.data(), N));
+        std::vector<int2> wl;
+        std::vector<int> wn;
+        wall_lists(h, W, wl, wn);
+        h->nwlinks = (int)wl.size();
+        h->nwnodes = (int)wn.size();
+        TRY(dev_alloc(h, &h->d_wlinks, sizeof(int2) * std::max<size_t>(1, wl.size())));
+        TRY(dev_alloc(h, &h->d_wnodes, sizeof(int) * std::max<size_t>(1, wn.size())));
+        if (!wl.empty()) TRY(upload(h, h->d_wlinks, wl.data(), sizeof(int2) * wl.size()));
+        if (!wn.empty()) TRY(upload(h, h->d_wnodes, wn.data(), sizeof(int) * wn.size()));
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) TRY(set_err(h, LBM_ERR_CUDA, "upload failed"));
     }
-    // tiles whose halo meets a wall node
-    std::vector<unsigned char> tflags(h->g.ntiles, 0);
-    std::vector<int> wtiles;
-    if (h->has_walls) {
-        const GridDesc& g = h->g;
-        for (int z = 0; z < h->n[2]; ++z)
-            for (int y = 0; y < h->n[1]; ++y)
-                for (int x = 0; x < h->n[0]; ++x) {
-                    if (!W[x + (long long)h->n[0] * (y + (long long)h->n[1] * z)]) continue;
-                    for (int dz = -1; dz <= 1; ++dz)
-                        for (int dy = -1; dy <= 1; ++dy)
-                            for (int dxx = -1; dxx <= 1; ++dxx) {
-                                if (h->dims == 2 && dz != 0) continue;
-                                const int xx = (x + dxx + h->n[0]) % h->n[0];
-                                const int yy = (y + dy + h->n[1]) % h->n[1];
-                                const int zz = (z + dz + h->n[2]) % h->n[2];
-                                const long long t = xx / g.t[0] + (long long)g.nt[0] * (yy / g.t[1] + (long long)g.nt[1] * (zz / g.t[2]));
-                                tflags[t] = 1;
-                            }
-                }
-        for (long long t = 0; t < g.ntiles; ++t)
-            if (tflags[t]) wtiles.push_back((int)t);
-    }
-    h->nwalltiles = (int)wtiles.size();
-    TRY(dev_alloc(h, &h->d_tileflags, h->g.ntiles));
-    TRY(upload(h, h->d_tileflags, tflags.data(), h->g.ntiles));
-    TRY(dev_alloc(h, &h->d_walltiles, sizeof(int) * std::max<size_t>(1, wtiles.size())));
-    if (!wtiles.empty()) TRY(upload(h, h->d_walltiles, wtiles.data(), sizeof(int) * wtiles.size()));
-    TRY(ensure_particle_capacity(h, 0, 0));
+    TRY(ensure_particle_capacity(h, 0));
 
     // force field, zeroed on walls (initMethods.jl:639-650)
-    std::vector<double> ff;
     if (cfg->force_mode == LBM_FORCE_FIELD) {
-        ff.assign(cfg->force_field, cfg->force_field + N * h->dims);
+        std::vector<double> ff(cfg->force_field, cfg->force_field + N * h->dims);
         if (h->has_walls)
             for (int k = 0; k < h->dims; ++k)
                 for (long long c = 0; c < N; ++c)
                     if (W[c]) ff[k * N + c] = 0.0;
         TRY(dev_alloc(h, &h->d_ffield, sizeof(double) * N * h->dims));
         TRY(upload(h, h->d_ffield, ff.data(), sizeof(double) * N * h->dims));
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) TRY(set_err(h, LBM_ERR_CUDA, "upload failed"));
     }
     // initial populations on the device (findInitialConditions)
     size_t need = 0;
@@ -656,9 +729,10 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
     ia.zero_walls = (h->has_walls || h->trt) ? 1 : 0;
     ia.force_mode = h->force_mode;
     h->ops.init(ia, h->stream);
-    CUDA_TRY(h, cudaGetLastError());
-    CUDA_TRY(h, cudaMemsetAsync(h->pop[1], 0, pop_bytes, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (cudaGetLastError() != cudaSuccess) TRY(set_err(h, LBM_ERR_CUDA, "initialisation kernel failed"));
+    if (cudaMemsetAsync(h->pop[1], 0, pop_bytes, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+        TRY(set_err(h, LBM_ERR_CUDA, "initialisation failed"));
 #undef TRY
     h->cur = 0;
     *out = h;
@@ -722,28 +796,45 @@ int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_ou
     P.coupleF = p->couple_forces ? 1 : 0;
     P.coupleT = p->couple_torques ? 1 : 0;
     P.valid = 0;
-    // partial-sum capacity: tiles covering the widest node box of the sphere
-    int cap = 1;
-    for (int a = 0; a < 3; ++a) {
-        int ta;
-        if (a >= d) {
-            ta = 1;
-        } else {
-            const int span = (int)std::floor(2.0 * p->radius / h->dx) + 8;
-            ta = std::min(h->g.nt[a], (span + h->g.t[a] - 1) / h->g.t[a] + 1);
-        }
-        cap *= ta;
+    for (int k = 0; k < 3; ++k) {
+        P.slo[k] = 1;
+        P.shi[k] = 0;
     }
-    long long off = 0;
-    for (const auto& q : h->hparts) off = std::max<long long>(off, (long long)q.part_off + q.part_cap);
-    P.part_off = (int)off;
-    P.part_cap = cap;
+    // capacities from the widest index box of the sphere: solid box <= 2r/dx + 5
+    // nodes per axis, near box (links) 2 more
+    long long span = (long long)std::floor(2.0 * p->radius / h->dx) + 6;
+    long long rows = 1, near = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a >= d) continue;
+        if (a > 0) rows *= std::min<long long>(span, h->n[a]);
+        near *= std::min<long long>(span + 2, h->n[a]);
+    }
+    if (near >= (1LL << 28)) return set_err(h, LBM_ERR_UNSUPPORTED, "particle too large for the link lists");
     const int pid = (int)h->hparts.size();
-    int rc = ensure_particle_capacity(h, pid + 1, off + cap);
+    long long ivl_off = 0, link_off = 0, part_off = 0;
+    for (const auto& q : h->hparts) {
+        ivl_off = std::max<long long>(ivl_off, (long long)q.ivl_off + q.ivl_cap);
+        link_off = std::max<long long>(link_off, (long long)q.link_off + q.link_cap);
+        part_off = std::max<long long>(part_off, (long long)q.part_off + (q.link_cap + kFixBlock - 1) / kFixBlock);
+    }
+    P.ivl_off = (int)ivl_off;
+    P.ivl_cap = (int)rows;
+    P.link_off = (int)link_off;
+    P.link_cap = (int)near;
+    P.part_off = (int)part_off;
+    P.nlinks = 0;
+    const long long chunks = (near + kFixBlock - 1) / kFixBlock;
+    int rc = ensure_particle_capacity(h, pid + 1);
+    if (rc) return rc;
+    rc = grow(h, &h->d_ivl, &h->ivl_slots, ivl_off + rows, ivl_off);
+    if (rc) return rc;
+    rc = grow(h, &h->d_links, &h->link_slots, link_off + near, link_off);
+    if (rc) return rc;
+    rc = grow(h, &h->d_partial, &h->partial_slots, (part_off + chunks) * kPartialStride, 0);
     if (rc) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(h->d_parts + pid, &P, sizeof(P), cudaMemcpyHostToDevice, h->stream));
     h->hparts.push_back(P);
-    h->maxtl = std::max(h->maxtl, cap);
+    h->maxchunks = std::max<int>(h->maxchunks, (int)chunks);
     drop_graphs(h);
     // initial setup: moveParticles!(initialSetup = true)
     h->ops.particles(particle_args(h, 1, pid), 1, h->stream);
@@ -764,7 +855,7 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
     while (nsteps - done >= kGraphSteps) {
         int rc = build_graph(h, h->cur);
         if (rc) return rc;
-        CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling ? 1 : 0][h->cur].exec, h->stream));
+        CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling >= 2 ? 1 : 0][h->cur].exec, h->stream));
         done += kGraphSteps;  // kGraphSteps is even: the buffer parity is unchanged
         slots_used = kGraphSteps;
     }
@@ -773,6 +864,7 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
         h->cur = 1 - h->cur;
         slots_used = std::max(slots_used, std::min(s + 1, kGraphSteps));
     }
+    join_particles(h);
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_end, h->stream));
     CUDA_TRY(h, cudaGetLastError());
     for (int64_t s = 0; s < nsteps; ++s) h->time += h->dt;
@@ -782,51 +874,37 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
     p = lbm_profile{};
     p.steps = nsteps;
     p.launches = nsteps * launches_per_tick(h);
+    p.bulk_cells = h->N;
     if (h->profiling && nsteps > 0) {
         float ms = 0;
         CUDA_TRY(h, cudaEventElapsedTime(&ms, h->t_begin, h->t_end));
         p.total_ms = ms;
-        const bool boundary = (long long)h->hparts.size() * h->maxtl + h->nwalltiles > 0;
-        double sb = 0, sbd = 0, sp = 0;
+        const bool fix = fixup_blocks(h) > 0;
+        double sb = 0, sf = 0, sp = 0;
+        if (h->profiling < 2) slots_used = 0;  // per-kernel events were not recorded
         for (int s = 0; s < slots_used; ++s) {
             CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 0), prof_event(h, s, 1)));
             sb += ms;
-            if (boundary) {
-                CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 2), prof_event(h, s, 3)));
-                sbd += ms;
+            if (fix) {
+                CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 1), prof_event(h, s, 2)));
+                sf += ms;
             }
             if (!h->hparts.empty()) {
-                // the particle kernel starts once both bulk and boundary have finished
-                float a = 0, b = 0;
-                CUDA_TRY(h, cudaEventElapsedTime(&a, prof_event(h, s, 1), prof_event(h, s, 4)));
-                if (boundary) CUDA_TRY(h, cudaEventElapsedTime(&b, prof_event(h, s, 3), prof_event(h, s, 4)));
-                sp += boundary ? std::min(a, b) : a;
+                CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 2), prof_event(h, s, 3)));
+                sp += ms;
             }
         }
-        p.bulk_ms = sb / slots_used;
-        p.boundary_ms = sbd / slots_used;
-        p.particles_ms = sp / slots_used;
+        p.bulk_ms = slots_used ? sb / slots_used : 0.0;
+        p.fixup_ms = slots_used ? sf / slots_used : 0.0;
+        p.particles_ms = slots_used ? sp / slots_used : 0.0;
         p.profiled_steps = slots_used;
-        // tiles the bulk kernel skipped in the last tick (particle bits or wall flags)
-        std::vector<unsigned long long> bits((size_t)h->g.ntiles * h->words);
-        std::vector<unsigned char> flags(h->g.ntiles);
-        CUDA_TRY(h, cudaMemcpy(bits.data(), h->d_tilebits, bits.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-        CUDA_TRY(h, cudaMemcpy(flags.data(), h->d_tileflags, flags.size(), cudaMemcpyDeviceToHost));
-        long long bcells = 0, btiles = 0;
-        const GridDesc& g = h->g;
-        for (long long t = 0; t < g.ntiles; ++t) {
-            bool b = flags[t] != 0;
-            for (int k = 0; k < h->words; ++k) b = b || bits[t * h->words + k] != 0;
-            if (!b) continue;
-            ++btiles;
-            const int tx = (int)(t % g.nt[0]), ty = (int)((t / g.nt[0]) % g.nt[1]), tz = (int)(t / ((long long)g.nt[0] * g.nt[1]));
-            const long long cx = std::min(g.t[0], g.n[0] - tx * g.t[0]);
-            const long long cy = std::min(g.t[1], g.n[1] - ty * g.t[1]);
-            const long long cz = std::min(g.t[2], g.n[2] - tz * g.t[2]);
-            bcells += cx * cy * cz;
+        long long entries = h->nwlinks;
+        if (!h->hparts.empty()) {
+            std::vector<ParticleDev> tmp(h->hparts.size());
+            CUDA_TRY(h, cudaMemcpy(tmp.data(), h->d_parts, sizeof(ParticleDev) * tmp.size(), cudaMemcpyDeviceToHost));
+            for (const auto& q : tmp) entries += near_volume(q, h->g, h->dims);
         }
-        p.bulk_cells = h->N - bcells;
-        p.boundary_tiles = btiles;
+        p.fixup_entries = entries;
     }
     return rc;
 }
@@ -835,12 +913,12 @@ int lbm_set_profiling(lbm_handle* h, int32_t on) {
     if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
     BIND(h);
     if (on && h->pev.empty()) {
-        h->pev.resize(5 * kGraphSteps);
+        h->pev.resize(4 * kGraphSteps);
         for (auto& e : h->pev) CUDA_TRY(h, cudaEventCreate(&e));
         CUDA_TRY(h, cudaEventCreate(&h->t_begin));
         CUDA_TRY(h, cudaEventCreate(&h->t_end));
     }
-    h->profiling = on != 0;
+    h->profiling = on < 0 ? 0 : (on > 2 ? 2 : on);
     return LBM_OK;
 }
 
@@ -848,6 +926,67 @@ int lbm_get_profile(lbm_handle* h, lbm_profile* out) {
     if (!h || !out) return set_err(h, LBM_ERR_INVALID, "null argument");
     *out = h->prof;
     return LBM_OK;
+}
+
+int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg_ms) {
+    if (!h || !avg_ms) return set_err(h, LBM_ERR_INVALID, "null argument");
+    if (kernel < LBM_KERNEL_BULK || kernel > LBM_KERNEL_PARTICLES || launches < 1)
+        return set_err(h, LBM_ERR_INVALID, "unknown kernel or launch count");
+    BIND(h);
+    const int np = (int)h->hparts.size();
+    if (kernel == LBM_KERNEL_FIXUP && fixup_blocks(h) == 0) return set_err(h, LBM_ERR_STATE, "model has no boundary links");
+    if (kernel == LBM_KERNEL_PARTICLES && np == 0) return set_err(h, LBM_ERR_STATE, "model has no particles");
+    // save everything the launches touch
+    const size_t pop_bytes = (size_t)h->N * h->q * storage_bytes(h->storage);
+    const size_t parts_b = sizeof(ParticleDev) * np, ivl_b = sizeof(int2) * h->ivl_slots,
+                 link_b = sizeof(int2) * h->link_slots, bits_b = sizeof(unsigned long long) * h->g.ntiles * h->words;
+    char* save = nullptr;
+    int rc = dev_alloc(h, &save, 2 * pop_bytes + parts_b + ivl_b + link_b + bits_b);
+    if (rc) return rc;
+    char* sp = save;
+    const void* srcs[6] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits};
+    const size_t sizes[6] = {pop_bytes, pop_bytes, parts_b, ivl_b, link_b, bits_b};
+    for (int k = 0; k < 6; ++k) {
+        if (sizes[k] && srcs[k]) CUDA_TRY(h, cudaMemcpyAsync(sp, srcs[k], sizes[k], cudaMemcpyDeviceToDevice, h->stream));
+        sp += sizes[k];
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(h, cudaEventCreate(&e0));
+    CUDA_TRY(h, cudaEventCreate(&e1));
+    int b = h->cur;
+    CUDA_TRY(h, cudaEventRecord(e0, h->stream));
+    for (int l = 0; l < launches; ++l) {
+        const StepArgs a = step_args(h, b);
+        if (kernel == LBM_KERNEL_BULK) {
+            if (use_vector_bulk(h))
+                h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
+            else
+                h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+            b = 1 - b;
+        } else if (kernel == LBM_KERNEL_FIXUP) {
+            h->ops.fixup(a, (unsigned)fixup_blocks(h), h->stream);
+        } else {
+            h->ops.particles(particle_args(h, 0, 0), (unsigned)np, h->stream);
+        }
+    }
+    CUDA_TRY(h, cudaEventRecord(e1, h->stream));
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *avg_ms = ms / launches;
+    sp = save;
+    void* dsts[6] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits};
+    for (int k = 0; k < 6; ++k) {
+        if (sizes[k] && dsts[k]) CUDA_TRY(h, cudaMemcpyAsync(dsts[k], sp, sizes[k], cudaMemcpyDeviceToDevice, h->stream));
+        sp += sizes[k];
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    dev_free(save);
+    h->device_bytes -= 2 * pop_bytes + parts_b + ivl_b + link_b + bits_b;
+    return check_device_error(h);
 }
 
 int lbm_get_fields(lbm_handle* h, double* rho, double* u) {
@@ -954,20 +1093,14 @@ int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask) {
     if (!h || !mask) return set_err(h, LBM_ERR_INVALID, "null argument");
     BIND(h);
     if (id < 1 || id > (int)h->hparts.size()) return set_err(h, LBM_ERR_INVALID, "no such particle");
-    ParticleDev P;
-    CUDA_TRY(h, cudaMemcpyAsync(&P, h->d_parts + (id - 1), sizeof(P), cudaMemcpyDeviceToHost, h->stream));
     int rc = ensure_tmp(h, h->N);
     if (rc) return rc;
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     MaskArgs m{};
     m.mask = reinterpret_cast<unsigned char*>(h->d_tmp);
-    for (int k = 0; k < 3; ++k) {
-        m.coord[k] = h->d_coord[k];
-        m.n[k] = h->n[k];
-        m.c[k] = P.mR[k];
-    }
+    m.part = h->d_parts + (id - 1);
+    m.ivl = h->d_ivl;
+    for (int k = 0; k < 3; ++k) m.n[k] = h->n[k];
     m.N = h->N;
-    m.r2 = P.r2;
     h->ops.mask(m, h->stream);
     CUDA_TRY(h, cudaGetLastError());
     CUDA_TRY(h, cudaMemcpyAsync(mask, m.mask, h->N, cudaMemcpyDeviceToHost, h->stream));
@@ -975,31 +1108,34 @@ int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask) {
     return LBM_OK;
 }
 
+// boundary links of the device solid region: fluid cells x with x - c_j solid
+// (periodic shift, bounceBackPrep), sorted by (direction, cell)
 int lbm_get_links(lbm_handle* h, int32_t id, int64_t* cells, int8_t* dirs, int64_t capacity, int64_t* n) {
     if (!h || !n) return set_err(h, LBM_ERR_INVALID, "null argument");
     std::vector<uint8_t> S(h->N);
     int rc = lbm_get_mask(h, id, S.data());
     if (rc) return rc;
     const HostLattice hl = host_lattice(h->lattice);
-    std::vector<std::vector<int64_t>> per(hl.q);
+    std::vector<std::vector<int64_t>> per(h->q);
     for (long long y = 0; y < h->N; ++y) {
         if (!S[y]) continue;
-        const int x0 = (int)(y % h->n[0]), y0 = (int)((y / h->n[0]) % h->n[1]), z0 = (int)(y / ((long long)h->n[0] * h->n[1]));
-        for (int i = 1; i < hl.q; ++i) {
-            const int xx = (x0 + hl.cx[i] + h->n[0]) % h->n[0];
-            const int yy = (y0 + hl.cy[i] + h->n[1]) % h->n[1];
-            const int zz = (z0 + hl.cz[i] + h->n[2]) % h->n[2];
+        const int x0 = (int)(y % h->n[0]), y0 = (int)((y / h->n[0]) % h->n[1]);
+        const int z0 = (int)(y / ((long long)h->n[0] * h->n[1]));
+        for (int j = 1; j < hl.q; ++j) {
+            const int xx = (x0 + hl.cx[j] + h->n[0]) % h->n[0];
+            const int yy = (y0 + hl.cy[j] + h->n[1]) % h->n[1];
+            const int zz = (z0 + hl.cz[j] + h->n[2]) % h->n[2];
             const long long x = xx + (long long)h->n[0] * (yy + (long long)h->n[1] * zz);
-            if (!S[x]) per[i].push_back(x);
+            if (!S[x]) per[j].push_back(x);
         }
     }
     int64_t k = 0;
-    for (int i = 0; i < hl.q; ++i) {
-        std::sort(per[i].begin(), per[i].end());
-        for (int64_t x : per[i]) {
+    for (int j = 0; j < h->q; ++j) {
+        std::sort(per[j].begin(), per[j].end());
+        for (int64_t x : per[j]) {
             if (cells && dirs && k < capacity) {
                 cells[k] = x;
-                dirs[k] = (int8_t)i;
+                dirs[k] = (int8_t)j;
             }
             ++k;
         }
@@ -1071,16 +1207,23 @@ int lbm_load_state(lbm_handle* h, const char* path) {
          (np == 0 || std::fread(parts.data(), sizeof(ParticleDev), np, fp) == (size_t)np);
     std::fclose(fp);
     if (!ok) return set_err(h, LBM_ERR_INVALID, "truncated checkpoint");
-    // clear the tile bits of the current geometry, then restore
+    // clear the tile bits of the current geometry, then restore and re-voxelise
     CUDA_TRY(h, cudaMemsetAsync(h->d_tilebits, 0, sizeof(unsigned long long) * h->g.ntiles * h->words, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->pop[h->cur], buf.data(), pop_bytes, cudaMemcpyHostToDevice, h->stream));
     for (int i = 0; i < np; ++i) {
-        parts[i].part_off = h->hparts[i].part_off;
-        parts[i].part_cap = h->hparts[i].part_cap;
+        const ParticleDev& hp = h->hparts[i];
+        parts[i].ivl_off = hp.ivl_off;
+        parts[i].ivl_cap = hp.ivl_cap;
+        parts[i].link_off = hp.link_off;
+        parts[i].link_cap = hp.link_cap;
+        parts[i].part_off = hp.part_off;
         parts[i].valid = 0;
+        for (int k = 0; k < 3; ++k) {
+            parts[i].slo[k] = 1;
+            parts[i].shi[k] = 0;
+        }
     }
     if (np) CUDA_TRY(h, cudaMemcpyAsync(h->d_parts, parts.data(), sizeof(ParticleDev) * np, cudaMemcpyHostToDevice, h->stream));
-    // re-voxelise from the restored state; the slip snapshot is restored as saved
     for (int i = 0; i < np; ++i) h->ops.particles(particle_args(h, 2, i), 1, h->stream);
     CUDA_TRY(h, cudaGetLastError());
     h->tick = tick;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "kernels.cuh"
+#include "fixup.cuh"
 #include "particles.cuh"
 #include "aux_kernels.cuh"
 
@@ -9,7 +10,8 @@ namespace lbm {
 
 struct Ops {
     void (*bulk)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
-    void (*boundary)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
+    void (*bulk_v4)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);  // null: not instantiated
+    void (*fixup)(const StepArgs&, unsigned grid, cudaStream_t);
     void (*particles)(const ParticleArgs&, unsigned grid, cudaStream_t);
     void (*encode)(const CodecArgs&, cudaStream_t);
     void (*decode)(const CodecArgs&, cudaStream_t);
@@ -18,7 +20,7 @@ struct Ops {
     void (*init)(const InitArgs&, cudaStream_t);
     void (*mask)(const MaskArgs&, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
-    const void* boundary_fn;
+    const void* fixup_fn;
 };
 
 inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -28,8 +30,11 @@ struct OpsImpl {
     static void bulk(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
         k_bulk<L, ST, TRT><<<grid, block, 0, s>>>(a);
     }
-    static void boundary(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
-        k_boundary<L, ST, TRT><<<grid, block, 0, s>>>(a);
+    static void bulk_v4(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
+        if constexpr (ST != ST_F64) k_bulk_v4<L, ST, TRT><<<grid, block, 0, s>>>(a);
+    }
+    static void fixup(const StepArgs& a, unsigned grid, cudaStream_t s) {
+        k_fixup<L, ST, TRT><<<grid, kFixBlock, 0, s>>>(a);
     }
     static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
         k_particles<L><<<grid, 256, 0, s>>>(a);
@@ -45,7 +50,8 @@ struct OpsImpl {
     static Ops make() {
         Ops o;
         o.bulk = bulk;
-        o.boundary = boundary;
+        o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
+        o.fixup = fixup;
         o.particles = particles;
         o.encode = encode;
         o.decode = decode;
@@ -54,7 +60,7 @@ struct OpsImpl {
         o.init = init;
         o.mask = mask;
         o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
-        o.boundary_fn = (const void*)k_boundary<L, ST, TRT>;
+        o.fixup_fn = (const void*)k_fixup<L, ST, TRT>;
         return o;
     }
 };

@@ -1,10 +1,20 @@
 // Particle update on the device: momentum-exchange reduction, Newton-Euler
-// integration with Rodrigues rotation, re-voxelisation bookkeeping.
-// Restates moveParticles! (src/gpu/particles.jl:7-92) for one particle per CTA.
+// integration with Rodrigues rotation, re-voxelisation and boundary-link
+// bookkeeping.  Restates moveParticles! (src/gpu/particles.jl:7-92), one
+// particle per CTA.
+//
+// The solid region of a particle (getSphere, src/gpu/aux.jl:206-215) is kept
+// as one x-interval per (y, z) row of its index box, each found with the exact
+// FP64 sphere test, so every membership query afterwards is two integer
+// compares.  The boundary links (bounceBackPrep, src/gpu/aux.jl:187-198) are
+// kept as a list of (fluid cell, direction mask) entries that is rebuilt only
+// when the intervals change; a sub-node move leaves both untouched.
 #pragma once
 #include "kernels.cuh"
 
 namespace lbm {
+
+constexpr int kIvlSmem = 2048;  // rows of solid intervals staged in shared memory
 
 struct ParticleArgs {
     ParticleDev* parts;
@@ -12,11 +22,11 @@ struct ParticleArgs {
     int mode;        // 0: tick update; 1: initial setup of particle `setup_pid`;
                      // 2: re-voxelise `setup_pid` keeping its slip snapshot (checkpoint restore)
     int setup_pid;
-    int pad;
+    int words;
     const double* partial;
     unsigned long long* tilebits;
-    int words;
-    int pad2;
+    int2* ivl;
+    int2* links;
     GridDesc g;
     const double* coord[3];
     double x0[3];
@@ -67,8 +77,7 @@ __device__ __forceinline__ void tile_bits_update(const ParticleArgs& a, const in
     const int total = tn[0] * tn[1] * tn[2];
     const unsigned long long bit = 1ull << (p & 63);
     const int word = p >> 6;
-    const int nthreads = blockDim.x;
-    for (int l = threadIdx.x; l < total; l += nthreads) {
+    for (int l = threadIdx.x; l < total; l += blockDim.x) {
         const int dx = l % tn[0], dy = (l / tn[0]) % tn[1], dz = l / (tn[0] * tn[1]);
         const long long tx = (tlo[0] + dx) % a.g.nt[0];
         const long long ty = (tlo[1] + dy) % a.g.nt[1];
@@ -80,21 +89,59 @@ __device__ __forceinline__ void tile_bits_update(const ParticleArgs& a, const in
     }
 }
 
+// exclusive prefix sum of one flag per thread over the CTA (256 threads)
+__device__ __forceinline__ int block_scan(int flag, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int v = flag;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    if (lane == 31) s_warp[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            const int t = s_warp[w];
+            s_warp[w] = run;
+            run += t;
+        }
+        s_warp[8] = run;
+    }
+    __syncthreads();
+    const int excl = s_warp[warp] + v - flag;
+    *total = s_warp[8];
+    __syncthreads();
+    return excl;
+}
+
 template <class L>
 __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
     constexpr int D = L::D;
     const int p = a.mode != 0 ? a.setup_pid : (int)blockIdx.x;
-    ParticleDev& P = a.parts[p];
     const int tid = threadIdx.x;
     __shared__ double s_red[8][6];
-    __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_cert;
+    __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty;
     __shared__ unsigned s_links;
+    __shared__ int s_warp[9];
+    __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
+    // the particle record is staged in shared memory: the update below is a
+    // serial chain of reads and writes that must not go to global memory
+    __shared__ ParticleDev sP;
+    static_assert(sizeof(ParticleDev) % 8 == 0, "ParticleDev is copied in 8-byte words");
+    {
+        const unsigned long long* gsrc = reinterpret_cast<const unsigned long long*>(a.parts + p);
+        unsigned long long* sdst = reinterpret_cast<unsigned long long*>(&sP);
+        for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += blockDim.x) sdst[k] = gsrc[k];
+    }
+    __syncthreads();
+    ParticleDev& P = sP;
 
-    // 1. momentum exchange: fixed-order reduction of the per-tile partials
+    // 1. momentum exchange: fixed-order reduction of the per-chunk partials
     double acc[6] = {0, 0, 0, 0, 0, 0};
     if (a.mode == 0) {
-        const int ntl = P.tn[0] * P.tn[1] * P.tn[2];
-        for (int l = tid; l < ntl; l += blockDim.x) {
+        const int nch = (near_volume(P, a.g, D) + kFixBlock - 1) / kFixBlock;
+        for (int l = tid; l < nch; l += blockDim.x) {
             const double* q = a.partial + (long long)(P.part_off + l) * kPartialStride;
             for (int k = 0; k < 6; ++k) acc[k] += q[k];
         }
@@ -105,8 +152,10 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
         for (int k = 0; k < 6; ++k) s_red[tid >> 5][k] = acc[k];
     __syncthreads();
 
-    // 2. Newton-Euler update (one thread, FP64)
-    if (tid == 0) {
+    // 2. Newton-Euler update in FP64: translation (thread 0) and rotation
+    //    (thread 32) are independent chains and run on different warps
+    __shared__ int s_alpha;
+    if (tid == 0 || tid == 32) {
         double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
         const int nw = blockDim.x >> 5;
         for (int k = 0; k < 3; ++k) {
@@ -115,16 +164,24 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
                 T[k] += s_red[w][3 + k];
             }
         }
-        bool moved = a.mode != 0, need_nv = a.mode == 1;
-        if (a.mode == 0) {
-            const double dt = a.dt;
-            if (P.coupleF) {
+        const double dt = a.dt;
+        if (tid == 0) {
+            bool moved = a.mode != 0;
+            if (a.mode == 0 && P.coupleF) {
                 for (int k = 0; k < D; ++k) P.v[k] = P.v[k] + dt * (F[k] * P.inv_mass);
                 for (int k = 0; k < D; ++k) P.R[k] = P.R[k] + dt * P.v[k];
                 for (int k = 0; k < D; ++k)
                     if (P.v[k] != 0.0) moved = true;
             }
-            if (P.coupleT) {
+            s_moved = moved ? 1 : 0;
+            if (a.mode != 2)
+                for (int k = 0; k < 3; ++k) {
+                    P.lastF[k] = F[k];
+                    P.lastT[k] = T[k];
+                }
+        } else {
+            bool alpha = false;
+            if (a.mode == 0 && P.coupleT) {
                 const int nw2 = D == 2 ? 1 : 3;
                 double Al[3] = {0, 0, 0};
                 for (int k = 0; k < nw2; ++k) Al[k] = T[k] * P.inv_inertia;
@@ -156,15 +213,15 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
                     }
                 }
                 for (int k = 0; k < nw2; ++k)
-                    if (Al[k] != 0.0) need_nv = true;
+                    if (Al[k] != 0.0) alpha = true;
             }
-            need_nv = need_nv || moved;
+            s_alpha = alpha ? 1 : 0;
         }
-        if (a.mode != 2)
-            for (int k = 0; k < 3; ++k) {
-                P.lastF[k] = F[k];
-                P.lastT[k] = T[k];
-            }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const bool moved = s_moved != 0;
+        const bool need_nv = a.mode == 1 || (a.mode == 0 && (moved || s_alpha));
         if (need_nv)
             for (int k = 0; k < 3; ++k) {
                 P.sR[k] = P.R[k];
@@ -173,9 +230,12 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
                 P.sE[k] = P.e[k];
             }
         s_moved = moved ? 1 : 0;
+        s_changed = (a.mode != 0 || !P.valid) ? 1 : 0;
+        s_bad = 0;
+        s_nonempty = 0;
         for (int k = 0; k < 3; ++k) {
             s_oldbox[k] = P.tlo[k];
-            s_oldbox[3 + k] = (a.mode != 0 && !P.valid) ? 0 : P.tn[k];
+            s_oldbox[3 + k] = P.valid ? P.tn[k] : 0;
         }
         if (moved) {
             for (int k = 0; k < 3; ++k) P.mR[k] = P.R[k];
@@ -183,69 +243,93 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
             solid_box(a, P.R, P.radius, D, lo, hi);
             bool empty = false;
             for (int k = 0; k < 3; ++k) {
+                if (lo[k] != P.slo[k] || hi[k] != P.shi[k]) s_changed = 1;
                 P.slo[k] = lo[k];
                 P.shi[k] = hi[k];
                 empty = empty || lo[k] > hi[k];
             }
+            int rows = empty ? 0 : (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+            if (rows > P.ivl_cap) {
+                atomicOr(a.err, kErrIntervalOverflow);
+                rows = 0;
+                empty = true;
+            }
+            s_rows = rows;
             int tlo[3] = {0, 0, 0}, tn[3] = {0, 0, 0};
             if (!empty)
                 for (int k = 0; k < 3; ++k)
                     tile_range(lo[k] - 1, hi[k] - lo[k] + 3, a.g.n[k], a.g.t[k], a.g.nt[k], &tlo[k], &tn[k]);
-            if (tn[0] * tn[1] * tn[2] > P.part_cap) {
-                atomicOr(a.err, kErrPartialOverflow);
-                tn[0] = tn[1] = tn[2] = 0;
-                empty = true;
-            }
             for (int k = 0; k < 3; ++k) {
                 P.tlo[k] = tlo[k];
                 P.tn[k] = tn[k];
                 s_newbox[k] = tlo[k];
                 s_newbox[3 + k] = tn[k];
             }
-            // boundary links exist in every moving direction when the sphere has
-            // a node and does not span a whole periodic axis; otherwise count
-            int cert = 0;
-            if (!empty) {
-                int nearest[3];
-                for (int k = 0; k < 3; ++k) {
-                    if (k >= D) {
-                        nearest[k] = 0;
-                        continue;
-                    }
-                    double c = rint((P.R[k] - a.x0[k]) / a.dx);
-                    c = c < 0.0 ? 0.0 : (c > (double)(a.g.n[k] - 1) ? (double)(a.g.n[k] - 1) : c);
-                    nearest[k] = (int)c;
-                }
-                const bool nonempty = sphere_test<D>(a.coord[0][nearest[0]], a.coord[1][nearest[1]],
-                                                     D == 3 ? a.coord[2][nearest[2]] : 0.0, P.R, P.r2);
-                bool spans = false;
-                for (int k = 0; k < D; ++k) spans = spans || (hi[k] - lo[k] + 1 >= a.g.n[k]);
-                cert = (nonempty && !spans) ? 1 : 0;
-            }
-            s_cert = empty ? 2 : cert;
         }
         P.valid = 1;
     }
     __syncthreads();
+    if (!s_moved) {
+        // nothing geometric changed; write the record back
+        const unsigned long long* ssrc = reinterpret_cast<const unsigned long long*>(&sP);
+        unsigned long long* gdst = reinterpret_cast<unsigned long long*>(a.parts + p);
+        for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += blockDim.x) gdst[k] = ssrc[k];
+        return;
+    }
 
-    // 3. tile bits of the candidate lists and exact link directions
-    if (s_moved) {
-        if (s_oldbox[3] * s_oldbox[4] * s_oldbox[5] > 0) tile_bits_update(a, s_oldbox, s_oldbox + 3, p, false);
-        __syncthreads();
-        if (s_newbox[3] * s_newbox[4] * s_newbox[5] > 0) tile_bits_update(a, s_newbox, s_newbox + 3, p, true);
-        if (tid == 0) {
-            if (s_cert == 1) {
-                unsigned m = 0;
-                for (int i = 1; i < L::Q; ++i) m |= 1u << i;
-                P.dirlinks = m;
-            } else if (s_cert == 2) {
-                P.dirlinks = 0u;
+    // 3. solid intervals of the new position, compared with the stored ones
+    {
+        const int lx0 = P.slo[0], lx1 = P.shi[0];
+        const int ly = P.shi[1] - P.slo[1] + 1;
+        int changed = 0;
+        for (int r = tid; r < s_rows; r += blockDim.x) {
+            const int y = P.slo[1] + r % ly;
+            const int z = P.slo[2] + r / ly;
+            const double Y = a.coord[1][y], Z = D == 3 ? a.coord[2][z] : 0.0;
+            int xlo = 1, xhi = 0;
+            for (int x = lx0; x <= lx1; ++x) {
+                if (sphere_test<D>(a.coord[0][x], Y, Z, P.mR, P.r2)) {
+                    if (xlo > xhi) xlo = x;
+                    xhi = x;
+                }
             }
-            s_links = 0u;
+            int2* slot = a.ivl + P.ivl_off + r;
+            const int2 old = *slot;
+            if (old.x != xlo || old.y != xhi) changed = 1;
+            *slot = make_int2(xlo, xhi);
+            if (r < kIvlSmem) s_ivl[r] = make_int2(xlo, xhi);
+            if (xlo <= xhi) s_nonempty = 1;
         }
-        __syncthreads();
-        if (s_cert == 0) {
-            // exact enumeration over the solid box (rare: tiny or domain-spanning spheres)
+        if (changed) atomicOr(&s_changed, 1);
+    }
+    __syncthreads();
+
+    // 4. boundary-link entries over the near box (solid box + 1, periodic)
+    const bool ivl_smem = s_rows <= kIvlSmem;
+    auto inS = [&](int x, int y, int z) -> bool {
+        if (!ivl_smem) return solid_at(P, a.ivl, x, y, z);
+        if (y < P.slo[1] || y > P.shi[1] || z < P.slo[2] || z > P.shi[2]) return false;
+        const int2 iv = s_ivl[(y - P.slo[1]) + (P.shi[1] - P.slo[1] + 1) * (z - P.slo[2])];
+        return x >= iv.x && x <= iv.y;
+    };
+    // Directions with at least one link (the break rule of fluids.jl:184).  A
+    // non-empty solid region that spans no periodic axis has a link in every
+    // moving direction (its extreme node along c_j always has a fluid
+    // neighbour); otherwise the links are counted exactly over the solid box.
+    if (s_changed) {
+        bool spans = false;
+        for (int k = 0; k < D; ++k) spans = spans || (P.shi[k] - P.slo[k] + 1 >= a.g.n[k]);
+        if (!s_nonempty) {
+            if (tid == 0) P.dirlinks = 0u;
+        } else if (!spans) {
+            if (tid == 0) {
+                unsigned m = 0;
+                for (int j = 1; j < L::Q; ++j) m |= 1u << j;
+                P.dirlinks = m;
+            }
+        } else {
+            if (tid == 0) s_links = 0u;
+            __syncthreads();
             const int l0 = P.shi[0] - P.slo[0] + 1, l1 = P.shi[1] - P.slo[1] + 1, l2 = P.shi[2] - P.slo[2] + 1;
             const long long vol = (long long)l0 * l1 * l2;
             unsigned m = 0;
@@ -253,21 +337,35 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
                 const int x = P.slo[0] + (int)(q % l0);
                 const int y = P.slo[1] + (int)((q / l0) % l1);
                 const int z = P.slo[2] + (int)(q / ((long long)l0 * l1));
-                if (!sphere_test<D>(a.coord[0][x], a.coord[1][y], D == 3 ? a.coord[2][z] : 0.0, P.mR, P.r2))
-                    continue;
+                if (!inS(x, y, z)) continue;
 #pragma unroll
-                for (int i = 1; i < L::Q; ++i) {
-                    const int tx = wrap_idx(x + L::cx(i), a.g.n[0]);
-                    const int ty = wrap_idx(y + L::cy(i), a.g.n[1]);
-                    const int tz = wrap_idx(z + L::cz(i), a.g.n[2]);
-                    if (!sphere_test<D>(a.coord[0][tx], a.coord[1][ty], D == 3 ? a.coord[2][tz] : 0.0, P.mR, P.r2))
-                        m |= 1u << i;
+                for (int j = 1; j < L::Q; ++j) {  // link (y + c_j, j): source y solid, target fluid
+                    const int tx = wrap_idx(x + L::cx(j), a.g.n[0]);
+                    const int ty = wrap_idx(y + L::cy(j), a.g.n[1]);
+                    const int tz = wrap_idx(z + L::cz(j), a.g.n[2]);
+                    if (!inS(tx, ty, tz)) m |= 1u << j;
                 }
             }
             if (m) atomicOr(&s_links, m);
             __syncthreads();
             if (tid == 0) P.dirlinks = s_links;
         }
+    }
+    __syncthreads();
+
+    // 5. candidate bits of the tiles around the particle
+    bool same = true;
+    for (int k = 0; k < 6; ++k) same = same && s_oldbox[k] == s_newbox[k];
+    if (!same) {
+        if (s_oldbox[3] * s_oldbox[4] * s_oldbox[5] > 0) tile_bits_update(a, s_oldbox, s_oldbox + 3, p, false);
+        __syncthreads();
+        if (s_newbox[3] * s_newbox[4] * s_newbox[5] > 0) tile_bits_update(a, s_newbox, s_newbox + 3, p, true);
+    }
+    __syncthreads();
+    {
+        const unsigned long long* ssrc = reinterpret_cast<const unsigned long long*>(&sP);
+        unsigned long long* gdst = reinterpret_cast<unsigned long long*>(a.parts + p);
+        for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += blockDim.x) gdst[k] = ssrc[k];
     }
 }
 

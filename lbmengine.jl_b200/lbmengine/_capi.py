@@ -117,13 +117,13 @@ class LbmProfile(C.Structure):
     _fields_ = [
         ("total_ms", C.c_double),
         ("bulk_ms", C.c_double),
-        ("boundary_ms", C.c_double),
+        ("fixup_ms", C.c_double),
         ("particles_ms", C.c_double),
         ("steps", C.c_int64),
         ("launches", C.c_int64),
         ("profiled_steps", C.c_int64),
         ("bulk_cells", C.c_int64),
-        ("boundary_tiles", C.c_int64),
+        ("fixup_entries", C.c_int64),
     ]
 
 
@@ -145,6 +145,7 @@ PROTOTYPES = [
     ("lbm_get_info", C.c_int, [C.c_void_p, C.POINTER(LbmInfo)]),
     ("lbm_set_profiling", C.c_int, [C.c_void_p, C.c_int32]),
     ("lbm_get_profile", C.c_int, [C.c_void_p, C.POINTER(LbmProfile)]),
+    ("lbm_time_kernel", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     ("lbm_save_state", C.c_int, [C.c_void_p, C.c_char_p]),
     ("lbm_load_state", C.c_int, [C.c_void_p, C.c_char_p]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),

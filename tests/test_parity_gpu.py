@@ -28,7 +28,7 @@ def _compare(res, gpu, orc, storage, tag):
     rho_g = gpu.massDensity.ravel(order="F")
     u_g = gpu.fluidVelocity.reshape(-1, res.dims, order="F").T
     assert rel_l2(rho_g, rho_o) <= tol["field"], f"{tag}: rho rel L2 {rel_l2(rho_g, rho_o):.3e}"
-    du = rel_l2(u_g, u_o)
+    du = rel_l2(u_g, u_o, floor=1e-4)  # velocities of the cases are O(1e-4 .. 1e-3)
     assert du <= tol["field"] * (10 if storage == "f32" else 1), f"{tag}: u rel L2 {du:.3e}"
     pg, po = gpu.particle_states(), orc.particles()
     assert len(pg) == len(po)
