@@ -237,6 +237,35 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
 int lbm_save_state(lbm_handle* h, const char* path);
 int lbm_load_state(lbm_handle* h, const char* path);
 
+/* Allocation-free stepping.  No counterpart in the reference.
+ *
+ * Same ticks and results as lbm_step, for callers that must not allocate
+ * device memory once their run has started: codes that reserve all device
+ * memory up front (another library's memory pool, a fixed per-process budget)
+ * and real-time or embedded hosts whose policy forbids allocation after
+ * initialisation.  lbm_step instantiates CUDA graphs on its first call and
+ * after every lbm_add_particle, which allocates; this entry point launches the
+ * kernels directly and keeps the fix-up kernel's momentum-exchange partials in
+ * a fixed device array compiled into the library (LBM_NOALLOC_SLOTS slots of
+ * 8 doubles = 1 MiB, held by every device that loads the library until the
+ * process exits) instead of the handle's buffer.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine.
+ *
+ * - The first call on a device looks up that array's device address
+ *   (cudaGetSymbolAddress) with the device current; make that first call before
+ *   any stream capture that the caller runs.
+ * - Models whose particles need more than LBM_NOALLOC_SLOTS partial slots
+ *   (one per particle and 64 near-box nodes) are rejected with
+ *   LBM_ERR_UNSUPPORTED; the message names both sizes.
+ * - All calls in the process share the array: calls that overlap on the GPU
+ *   (two handles stepped concurrently on the same device) race and must be
+ *   serialised by the caller.  The used slots are cleared at the start of
+ *   every call; nothing else carries over between calls.
+ * - The model itself (populations, particle records) is allocated earlier,
+ *   by lbm_create and lbm_add_particle. */
+#define LBM_NOALLOC_SLOTS 16384
+int lbm_step_noalloc(lbm_handle* h, int64_t nsteps);
+
 const char* lbm_last_error(lbm_handle* h);
 const char* lbm_last_global_error(void);
 void lbm_destroy(lbm_handle* h);

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1228,6 +1229,165 @@ int lbm_load_state(lbm_handle* h, const char* path) {
     CUDA_TRY(h, cudaGetLastError());
     h->tick = tick;
     h->time = time;
+    return check_device_error(h);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free stepping (lbm_step_noalloc)
+// ---------------------------------------------------------------------------
+namespace {
+
+// Momentum-exchange partials of lbm_step_noalloc, compiled into the library
+// image: LBM_NOALLOC_SLOTS slots of kPartialStride doubles (1 MiB) that every
+// device loading the library holds until the process exits.  In host code
+// this name only stands for the symbol; the kernels get the device address
+// that cudaGetSymbolAddress returns for the current device.
+static __device__ __align__(256) double g_noalloc_partials[LBM_NOALLOC_SLOTS * kPartialStride];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// device address of g_noalloc_partials on the handle's device (current after BIND)
+int noalloc_scratch(lbm_handle* h, double** out) {
+    if (h->device < 0 || h->device >= kNoallocMaxDevices)
+        return set_err(h, LBM_ERR_UNSUPPORTED, "lbm_step_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[h->device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return set_err(h, LBM_ERR_CUDA,
+                           std::string("lbm_step_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        }
+        g_noalloc_addr[h->device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[h->device];
+    return LBM_OK;
+}
+
+template <class L>
+void noalloc_lattice_of(int* cx, int* cy, int* cz, int* q) {
+    *q = L::Q;
+    for (int i = 0; i < L::Q; ++i) {
+        cx[i] = L::cx(i);
+        cy[i] = L::cy(i);
+        cz[i] = L::cz(i);
+    }
+}
+
+// the StepArgs of step_args(), built without host heap use and with the
+// partial sums redirected to `partial`
+StepArgs noalloc_step_args(const lbm_handle* h, int src, double* partial) {
+    int cx[27], cy[27], cz[27], q = 0;
+    switch (h->lattice) {
+        case LBM_D2Q9: noalloc_lattice_of<D2Q9>(cx, cy, cz, &q); break;
+        case LBM_D3Q15: noalloc_lattice_of<D3Q15>(cx, cy, cz, &q); break;
+        case LBM_D3Q19: noalloc_lattice_of<D3Q19>(cx, cy, cz, &q); break;
+        default: noalloc_lattice_of<D3Q27>(cx, cy, cz, &q); break;
+    }
+    StepArgs a{};
+    a.src = h->pop[src];
+    a.dst = h->pop[1 - src];
+    a.g = h->g;
+    for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
+    a.tilebits = h->d_tilebits;
+    a.words = h->words;
+    a.nparts = (int)h->hparts.size();
+    a.wall = h->d_wall;
+    a.uw = h->d_uw;
+    a.ffield = h->d_ffield;
+    a.parts = h->d_parts;
+    a.ivl = h->d_ivl;
+    a.links = h->d_links;
+    a.wlinks = h->d_wlinks;
+    a.wnodes = h->d_wnodes;
+    a.nwlinks = h->nwlinks;
+    a.nwnodes = h->nwnodes;
+    a.maxchunks = h->maxchunks;
+    a.partial = partial;
+    a.err = h->d_err;
+    a.rho0 = h->rho0;
+    a.scale = h->scale;
+    a.inv_scale = 1.0 / h->scale;
+    a.omega = h->dt / h->tau;
+    a.omega_p = h->dt / h->tau;
+    a.omega_m = h->trt ? h->dt / h->tau_minus : 0.0;
+    a.guo_k = h->dt * (1 - h->dt / (2 * h->tau));
+    a.guo_kp = a.guo_k;
+    a.guo_km = h->trt ? h->dt * (1 - h->dt / (2 * h->tau_minus)) : 0.0;
+    for (int k = 0; k < 3; ++k) a.F[k] = h->F[k];
+    a.half_dt = 0.5 * h->dt;
+    a.coeff = std::pow(h->dx, h->dims) / h->dt;
+    a.force_mode = h->force_mode;
+    a.incompressible = h->incompressible;
+    a.rho_inc = h->rho_inc;
+    const double kodd = h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k;
+    const double keven = h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k;
+    a.gK0 = h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k;
+    a.gkA = kodd;
+    a.gkB = keven;
+    const size_t esz = storage_bytes(h->storage);
+    for (int i = 0; i < 27; ++i) {
+        a.gA[i] = a.gB[i] = 0.0;
+        a.srcq[i] = nullptr;
+        a.dstq[i] = nullptr;
+    }
+    for (int i = 0; i < q; ++i) {
+        const double cF = cx[i] * h->F[0] + cy[i] * h->F[1] + cz[i] * h->F[2];
+        a.gA[i] = kodd * cF;
+        a.gB[i] = keven * cF;
+        a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
+        a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
+    }
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+// lbm_step without allocation: direct launches on the handle's stream, the
+// fix-up partials in g_noalloc_partials (see include/lbm_b200.h)
+int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (nsteps < 0) return set_err(h, LBM_ERR_INVALID, "ticks must be non-negative");
+    BIND(h);
+    long long slots = 0;  // partial slots the particles use: max(part_off + chunks)
+    for (const ParticleDev& q : h->hparts)
+        slots = std::max<long long>(slots, (long long)q.part_off + (q.link_cap + kFixBlock - 1) / kFixBlock);
+    if (slots > LBM_NOALLOC_SLOTS) {
+        char msg[192];
+        std::snprintf(msg, sizeof(msg),
+                      "lbm_step_noalloc: the particles need %lld momentum-exchange slots; the fixed array holds %d",
+                      slots, LBM_NOALLOC_SLOTS);
+        return set_err(h, LBM_ERR_UNSUPPORTED, msg);
+    }
+    double* scratch = nullptr;
+    int rc = noalloc_scratch(h, &scratch);
+    if (rc) return rc;
+    if (slots > 0)  // slots used by this model start from zero in every call
+        CUDA_TRY(h, cudaMemsetAsync(scratch, 0, sizeof(double) * kPartialStride * slots, h->stream));
+    ParticleArgs pa = particle_args(h, 0, 0);
+    pa.partial = scratch;
+    const long long nb = fixup_blocks(h);
+    const int np = (int)h->hparts.size();
+    for (int64_t s = 0; s < nsteps; ++s) {
+        const StepArgs a = noalloc_step_args(h, h->cur, scratch);
+        if (use_vector_bulk(h))
+            h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
+        else
+            h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+        if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
+        if (np > 0) h->ops.particles(pa, (unsigned)np, h->stream);
+        h->cur = 1 - h->cur;
+    }
+    CUDA_TRY(h, cudaGetLastError());
+    for (int64_t s = 0; s < nsteps; ++s) h->time += h->dt;
+    h->tick += nsteps;
     return check_device_error(h);
 }
 

@@ -148,6 +148,7 @@ PROTOTYPES = [
     ("lbm_time_kernel", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     ("lbm_save_state", C.c_int, [C.c_void_p, C.c_char_p]),
     ("lbm_load_state", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("lbm_step_noalloc", C.c_int, [C.c_void_p, C.c_int64]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_last_global_error", C.c_char_p, []),
     ("lbm_destroy", None, [C.c_void_p]),
