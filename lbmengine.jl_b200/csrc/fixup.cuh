@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
         load_collide<L, ST, TRT>(a, cell, true, s);
         rhoL = (double)s.rho;  // rho^n(x), the density of model.massDensity
 #pragma unroll
-        for (int i = 0; i < Q; ++i) s_g[i][tid] = s.g[i];
+        for (int i = 0; i < Q; ++i) s_g[i][tid] = s.g[i] * R(a.inv_scale);  // storage -> f/w - rho0
     }
 
     double acc[6] = {0, 0, 0, 0, 0, 0};

@@ -177,19 +177,26 @@ __device__ __forceinline__ void slip_velocity(const double* sR, const double* sV
 
 // ---------------------------------------------------------------------------
 // Collision of one node (collisionStep + guoForcingTerm, src/gpu/fluids.jl:58-127)
-// on the shifted, weight-normalised populations g_i = f_i/w_i - rho0, in place.
+// on the shifted, weight-normalised populations, in place.  The values are in
+// storage units g'_i = S (f_i/w_i - rho0), S = a.scale (1 for FP32/FP64, a
+// power of two for FP16/BF16), so no per-value rescaling is needed.
 // Returns rho^n (the density the reference holds in model.massDensity).
 //
-// With m = rho (rho_inc for the incompressible equilibrium) and c.u = cu:
-//   g_eq_i = (rho - rho0) - 1.5 m u.u + 4.5 m cu^2 + 3 m cu
-//   Guo/w_i: BGK  A_i + K0 + B_i cu   (A_i = 3k c.F, B_i = 9k c.F, K0 = -3k u.F)
-//            TRT  even K0 + B_i cu (k = k+), odd A_i (k = k-)
-// A_i and B_i are per-direction constants for a uniform force (host-computed).
+// With m = rho (rho_inc for the incompressible equilibrium) and cu = c_i.u:
+//   g_eq_i/S = (rho - rho0) - 1.5 m u.u + 4.5 m cu^2 + 3 m cu
+//   Guo/(w_i S): BGK  A_i + K0 + B_i cu   (A_i = 3k c.F, B_i = 9k c.F, K0 = -3k u.F)
+//                TRT  even K0 + B_i cu (k = k+), odd A_i (k = k-)
+// A_i, B_i (and the K0 coefficient) arrive pre-multiplied by S.  For a pair
+// (i, opp(i)) = (a, b) the update is
+//   TRT: a* = (1-h+-h-) a + (h- - h+) b + E + O,  b* = (1-h+-h-) b + (h- - h+) a + E - O
+//   BGK: a* = (1-w) a + E + O,                    b* = (1-w) b + E - O
+// with E the even part (relaxed symmetric equilibrium + even Guo term) and O
+// the odd part, h+- = omega+-/2.
 // ---------------------------------------------------------------------------
 template <class L, class R, bool TRT>
 __device__ __forceinline__ R collide(const StepArgs& a, R* g, R Fx, R Fy, R Fz, bool field) {
     constexpr int Q = L::Q;
-    R drho = 0, jx = 0, jy = 0, jz = 0;
+    R drho = 0, jx = 0, jy = 0, jz = 0;  // S (rho - rho0), S (j - dt/2 F)
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         drho = fma(R(L::w(i)), g[i], drho);
@@ -197,11 +204,12 @@ __device__ __forceinline__ R collide(const StepArgs& a, R* g, R Fx, R Fy, R Fz, 
         if (L::cy(i) != 0) jy = fma(R(L::w(i) * L::cy(i)), g[i], jy);
         if (L::cz(i) != 0) jz = fma(R(L::w(i) * L::cz(i)), g[i], jz);
     }
-    const R rho = R(a.rho0) + drho;
+    const R S = R(a.scale), invS = R(a.inv_scale);
+    const R rho = fma(drho, invS, R(a.rho0));
     const R hdt = R(a.half_dt);
-    jx = fma(hdt, Fx, jx);
-    jy = fma(hdt, Fy, jy);
-    jz = fma(hdt, Fz, jz);
+    jx = fma(jx, invS, hdt * Fx);
+    jy = fma(jy, invS, hdt * Fy);
+    jz = fma(jz, invS, hdt * Fz);
     R ux = 0, uy = 0, uz = 0;
     if (rho != R(0)) {  // findFluidVelocity: u = 0 where rho == 0
         const R inv = R(1) / rho;
@@ -211,62 +219,50 @@ __device__ __forceinline__ R collide(const StepArgs& a, R* g, R Fx, R Fy, R Fz, 
     }
     const R usq = ux * ux + uy * uy + uz * uz;
     const R uF = ux * Fx + uy * Fy + uz * Fz;
-    const R rq = a.incompressible ? R(a.rho_inc) : rho;
-    const R c45 = R(4.5) * rq, c3 = R(3) * rq;
-    const R E0 = drho - R(1.5) * rq * usq;
+    const R Srq = S * (a.incompressible ? R(a.rho_inc) : rho);
+    const R E0 = fma(R(-1.5) * Srq, usq, drho);  // S (g_eq even part at cu = 0)
     const R K0 = R(a.gK0) * uF;
     const R kA = R(a.gkA), kB = R(a.gkB);
-    if (!TRT) {
-        const R om = R(a.omega), om1 = R(1) - om;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const int ib = L::opp(i);
-            if (ib < i) continue;
-            if (ib == i) {
-                g[i] = fma(om1, g[i], fma(om, E0, K0));
-                continue;
-            }
-            const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-            R A = R(a.gA[i]), B = R(a.gB[i]);
-            if (field) {
-                const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-                A = kA * cF;
-                B = kB * cF;
-            }
-            const R even = fma(c45, cu * cu, E0);
-            const R odd = c3 * cu;
-            const R Ge = fma(B, cu, K0);
-            g[i] = fma(om1, g[i], fma(om, even + odd, Ge + A));
-            g[ib] = fma(om1, g[ib], fma(om, even - odd, Ge - A));
-        }
-    } else {
+    R hsum, hdif, e0, k45, k3;  // pair coefficients
+    if (TRT) {
         const R omp = R(a.omega_p), omm = R(a.omega_m);
-        const R hp = R(0.5) * omp, hm = R(0.5) * omm;
+        hsum = R(1) - R(0.5) * (omp + omm);
+        hdif = R(0.5) * (omm - omp);
+        e0 = fma(omp, E0, K0);
+        k45 = omp * R(4.5) * Srq;
+        k3 = omm * R(3) * Srq;
+    } else {
+        const R om = R(a.omega);
+        hsum = R(1) - om;
+        hdif = R(0);
+        e0 = fma(om, E0, K0);
+        k45 = om * R(4.5) * Srq;
+        k3 = om * R(3) * Srq;
+    }
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const int ib = L::opp(i);
-            if (ib < i) continue;
-            if (ib == i) {
-                g[i] = g[i] - fma(omp, g[i] - E0, -K0);
-                continue;
-            }
-            const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-            R A = R(a.gA[i]), B = R(a.gB[i]);
-            if (field) {
-                const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-                A = kA * cF;
-                B = kB * cF;
-            }
-            const R ep = fma(c45, cu * cu, E0);  // symmetric part of g_eq
-            const R em = c3 * cu;                // antisymmetric part
-            const R Gp = fma(B, cu, K0);
-            const R s = g[i] + g[ib], d = g[i] - g[ib];
-            const R P = fma(hp, s, -fma(omp, ep, Gp));  // omega+ (g+ - g+eq) - G+
-            const R M = fma(hm, d, -fma(omm, em, A));   // omega- (g- - g-eq) - G-
-            const R gi = g[i] - P - M;
-            const R gb = g[ib] - P + M;
-            g[i] = gi;
-            g[ib] = gb;
+    for (int i = 0; i < Q; ++i) {
+        const int ib = L::opp(i);
+        if (ib < i) continue;
+        if (ib == i) {  // rest direction: a* = (1 - omega+) a + e0
+            g[i] = fma(TRT ? R(1) - R(a.omega_p) : hsum, g[i], e0);
+            continue;
+        }
+        const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
+        R A = R(a.gA[i]), B = R(a.gB[i]);
+        if (field) {
+            const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
+            A = kA * cF;
+            B = kB * cF;
+        }
+        const R E = fma(fma(k45, cu, B), cu, e0);
+        const R O = fma(k3, cu, A);
+        const R ga = g[i], gb = g[ib];
+        if (TRT) {
+            g[i] = fma(hsum, ga, fma(hdif, gb, E + O));
+            g[ib] = fma(hsum, gb, fma(hdif, ga, E - O));
+        } else {
+            g[i] = fma(hsum, ga, E + O);
+            g[ib] = fma(hsum, gb, E - O);
         }
     }
     return rho;
@@ -287,9 +283,8 @@ __device__ __forceinline__ void load_collide(const StepArgs& a, int cell, bool v
     constexpr int Q = L::Q;
     const T* __restrict__ src = static_cast<const T*>(a.src);
     const long long N = a.g.N;
-    const R inv_scale = R(a.inv_scale);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) s.g[i] = valid ? SS::dec(src[i * N + cell], inv_scale) : R(0);
+    for (int i = 0; i < Q; ++i) s.g[i] = valid ? SS::dec(src[i * N + cell], R(1)) : R(0);
     R Fx = 0, Fy = 0, Fz = 0;
     if (a.force_mode == 1) {
         Fx = R(a.F[0]);
@@ -331,11 +326,10 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
     const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
     T* __restrict__ dst = static_cast<T*>(a.dst);
     const long long N = a.g.N;
-    const R scale = R(a.scale);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int t = xs[L::cx(i) + 1] + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
-        dst[i * N + t] = SS::enc(s.g[i], scale);
+        dst[i * N + t] = SS::enc(s.g[i], R(1));
     }
 }
 
@@ -349,24 +343,24 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
 // ---------------------------------------------------------------------------
 template <int ST> struct Vec4;
 template <> struct Vec4<ST_F32> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v, float) {
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
         const float4 q = __ldcs(reinterpret_cast<const float4*>(static_cast<const float*>(base) + cell0));
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3, float) {
+    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
         *reinterpret_cast<float4*>(static_cast<float*>(base) + cell0) = make_float4(a0, a1, a2, a3);
     }
 };
 template <> struct Vec4<ST_F16> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v, float inv_scale) {
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
         const uint2 q = __ldcs(reinterpret_cast<const uint2*>(static_cast<const __half*>(base) + cell0));
         const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
         const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
-        v[0] = lo.x * inv_scale; v[1] = lo.y * inv_scale; v[2] = hi.x * inv_scale; v[3] = hi.y * inv_scale;
+        v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3, float scale) {
-        const __half2 lo = __floats2half2_rn(a0 * scale, a1 * scale);
-        const __half2 hi = __floats2half2_rn(a2 * scale, a3 * scale);
+    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
+        const __half2 lo = __floats2half2_rn(a0, a1);
+        const __half2 hi = __floats2half2_rn(a2, a3);
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
@@ -374,15 +368,15 @@ template <> struct Vec4<ST_F16> {
     }
 };
 template <> struct Vec4<ST_BF16> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v, float inv_scale) {
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
         const uint2 q = __ldcs(reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + cell0));
         const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.x));
         const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.y));
-        v[0] = lo.x * inv_scale; v[1] = lo.y * inv_scale; v[2] = hi.x * inv_scale; v[3] = hi.y * inv_scale;
+        v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3, float scale) {
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(a0 * scale, a1 * scale);
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(a2 * scale, a3 * scale);
+    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(a0, a1);
+        const __nv_bfloat162 hi = __floats2bfloat162_rn(a2, a3);
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
@@ -423,12 +417,11 @@ __global__ void __launch_bounds__(kBlockV4) k_bulk_v4(const StepArgs a) {
     const bool valid = y < ny;
     const int x0 = 4 * j;
     const int cell0 = valid ? x0 + nx * (y + ny * z) : 0;
-    const R inv_scale = R(a.inv_scale), scale = R(a.scale);
     R g[4][Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         R v[4] = {0, 0, 0, 0};
-        if (valid) Vec4<ST>::load(a.srcq[i], cell0, v, inv_scale);
+        if (valid) Vec4<ST>::load(a.srcq[i], cell0, v);
         g[0][i] = v[0];
         g[1][i] = v[1];
         g[2][i] = v[2];
@@ -453,11 +446,11 @@ __global__ void __launch_bounds__(kBlockV4) k_bulk_v4(const StepArgs a) {
     for (int i = 0; i < Q; ++i) {
         const int t0 = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
         if (L::cx(i) == 0) {
-            Vec4<ST>::store(a.dstq[i], t0, g[0][i], g[1][i], g[2][i], g[3][i], scale);
+            Vec4<ST>::store(a.dstq[i], t0, g[0][i], g[1][i], g[2][i], g[3][i]);
         } else if (L::cx(i) == 1) {
-            Vec4<ST>::store(a.dstq[i], t0, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i], scale);
+            Vec4<ST>::store(a.dstq[i], t0, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i]);
         } else {
-            Vec4<ST>::store(a.dstq[i], t0, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right], scale);
+            Vec4<ST>::store(a.dstq[i], t0, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right]);
         }
     }
 }

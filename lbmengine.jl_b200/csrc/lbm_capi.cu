@@ -245,9 +245,10 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.incompressible = h->incompressible;
     a.rho_inc = h->rho_inc;
     // Guo constants (collide(): BGK A_i + K0 + B_i cu ; TRT even K0 + B_i cu, odd A_i)
-    const double kodd = h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k;
-    const double keven = h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k;
-    a.gK0 = h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k;
+    // in storage units: collide() works on g' = S (f/w - rho0)
+    const double kodd = (h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k) * h->scale;
+    const double keven = (h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k) * h->scale;
+    a.gK0 = (h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k) * h->scale;
     a.gkA = kodd;
     a.gkB = keven;
     const HostLattice hl = host_lattice(h->lattice);
@@ -1325,9 +1326,10 @@ StepArgs noalloc_step_args(const lbm_handle* h, int src, double* partial) {
     a.force_mode = h->force_mode;
     a.incompressible = h->incompressible;
     a.rho_inc = h->rho_inc;
-    const double kodd = h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k;
-    const double keven = h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k;
-    a.gK0 = h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k;
+    // in storage units: collide() works on g' = S (f/w - rho0)
+    const double kodd = (h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k) * h->scale;
+    const double keven = (h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k) * h->scale;
+    a.gK0 = (h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k) * h->scale;
     a.gkA = kodd;
     a.gkB = keven;
     const size_t esz = storage_bytes(h->storage);
