@@ -68,6 +68,19 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def bulk_traffic(storage, cells):
+    """DRAM bytes per bulk launch from the ncu capture summarised in profiles/bulk_traffic.txt."""
+    path = os.path.join(REPO, "profiles", "bulk_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) == 2 and parts[0] == storage and not line.startswith("#"):
+                return round(float(parts[1]) * cells)
+    except OSError:
+        pass
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle sampling during the timed region."""
 
@@ -248,15 +261,7 @@ def run_ours(args):
     bulk_bytes = prof.bulk_cells * 2 * q * bpp
     achieved = bulk_bytes / (kern["bulk"] / 1e3) / 1e9 if kern["bulk"] else None
     peak, peak_kind = measured_peak()
-    traffic = None
-    tr_path = os.path.join(REPO, "profiles", "bulk_traffic.json")
-    if os.path.exists(tr_path):
-        try:
-            tr = json.load(open(tr_path)).get(f"{storage}", None)
-            if tr:
-                traffic = round(tr["dram_bytes_per_cell"] * prof.bulk_cells)
-        except Exception:
-            traffic = None
+    traffic = bulk_traffic(storage, prof.bulk_cells)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
                 "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"

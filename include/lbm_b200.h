@@ -99,8 +99,20 @@ typedef struct lbm_config {
     double rho_ref;            /* shift density rho0 of the stored populations (0 -> 1.0) */
     double store_scale;        /* power-of-two scale for F16/BF16 storage (0 -> default 2^12) */
     int32_t device;            /* CUDA device ordinal; < 0: the calling thread's current device */
-    int32_t reserved0;
+    int32_t schedule;          /* LBM_SCHEDULE_*: how the kernels of a tick are launched */
 } lbm_config;
+
+/* Kernel schedule of a tick.  Results do not depend on it (the per-node
+ * arithmetic is the same).
+ *   STREAM      bulk -> fix-up in stream order, particle update on a side
+ *               stream overlapping the next bulk pass (AUTO: the default)
+ *   PERSISTENT  one persistent kernel per tick over a work queue of bulk
+ *               tiles, fix-up blocks and particle updates (vector bulk kernel
+ *               with rows of at most 256 nodes; otherwise STREAM)
+ * (value 2 is reserved) */
+#define LBM_SCHEDULE_AUTO 0
+#define LBM_SCHEDULE_STREAM 1
+#define LBM_SCHEDULE_PERSISTENT 3
 
 /* ---- particle parameters: the resolved keyword set of addBead!/addSquirmer!
  * Replaces src/gpu/initMethods.jl:7-89 and :91-222.  The shim resolves B1/B2
@@ -208,7 +220,8 @@ int lbm_get_info(lbm_handle* h, lbm_info* info);
  * tracing (only a `verbose` progress print, src/gpu/fluids.jl:229-253). */
 typedef struct lbm_profile {
     double total_ms;        /* device time of the whole lbm_step call */
-    double bulk_ms;         /* mean duration of one bulk stream-collide launch */
+    double bulk_ms;         /* mean duration of one bulk stream-collide launch (of the whole tick
+                               kernel where bulk, fix-up and particles run as one persistent kernel) */
     double fixup_ms;        /* mean duration of one boundary-link fix-up launch (0 if none) */
     double particles_ms;    /* mean duration of one particle-update launch (0 if none) */
     int64_t steps;          /* ticks in the call */
@@ -224,13 +237,16 @@ int lbm_set_profiling(lbm_handle* h, int32_t level);
 int lbm_get_profile(lbm_handle* h, lbm_profile* out);
 
 /* Mean device duration of one launch of a single kernel of the tick
- * (0: bulk stream-collide, 1: boundary-link fix-up, 2: particle update),
- * from CUDA events around `launches` back-to-back launches on the handle's
- * stream.  The model state is saved before and restored after, so the
- * simulation is unaffected.  No counterpart in the reference. */
+ * (0: bulk stream-collide over all tiles, 1: boundary-link fix-up, 2:
+ * particle update, 3: the persistent tick kernel that runs all three as one
+ * launch; LBM_ERR_STATE where that kernel does not apply), from CUDA events
+ * around `launches` back-to-back launches on the handle's stream.  The model
+ * state is saved before and restored after, so the simulation is
+ * unaffected.  No counterpart in the reference. */
 #define LBM_KERNEL_BULK 0
 #define LBM_KERNEL_FIXUP 1
 #define LBM_KERNEL_PARTICLES 2
+#define LBM_KERNEL_TICK 3
 int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg_ms);
 
 /* Raw checkpoint of populations + particle FP64 state + tick/time. */

@@ -23,10 +23,11 @@
 
 namespace lbm {
 
-constexpr int kFixIvl = 1024;  // particle interval rows staged in shared memory
+constexpr int kFixIvl = 512;    // particle interval rows staged in shared memory
+constexpr int kFixCoord = 64;   // near-box node coordinates staged per axis
 
 template <class L, int ST, bool TRT>
-__global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
+__device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b) {
     using SS = Store<ST>;
     using T = typename SS::T;
     using R = typename SS::R;
@@ -39,9 +40,9 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
     __shared__ double s_red[kFixBlock / 32][6];
     __shared__ ParticleDev sP;
     __shared__ int2 s_ivl[kFixIvl];
+    __shared__ double s_X[3][kFixCoord];
     __shared__ int s_alone;
     const int tid = threadIdx.x;
-    const long long b = blockIdx.x;
     const long long npb = (long long)a.nparts * a.maxchunks;
     const long long nwlb = (a.nwlinks + kFixBlock - 1) / kFixBlock;
     T* __restrict__ dst = static_cast<T*>(a.dst);
@@ -103,15 +104,27 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
         }
     }
     if (is_part && a.wall && tid == 0) s_alone = 0;
-    // the owner's solid intervals
+    // the owner's solid intervals and near-box coordinates
     int rows = 0, ly = 1;
+    int ext[3] = {1, 1, 1};
+    if (is_part)
+        for (int k = 0; k < D; ++k) ext[k] = near_extent(sP, a.g, k, D);
+    const bool cst = is_part && ext[0] <= kFixCoord && ext[1] <= kFixCoord && ext[2] <= kFixCoord;
     if (is_part) {
         ly = sP.shi[1] - sP.slo[1] + 1;
         rows = ly * (sP.shi[2] - sP.slo[2] + 1);
         if (rows <= kFixIvl)
             for (int r = tid; r < rows; r += kFixBlock) s_ivl[r] = a.ivl[sP.ivl_off + r];
+        if (cst)
+            for (int k = 0; k < D; ++k)
+                for (int i = tid; i < ext[k]; i += kFixBlock)
+                    s_X[k][i] = a.coord[k][wrap_idx(sP.slo[k] - 1 + i, a.g.n[k])];
     }
     __syncthreads();
+    // coordinate of node index i on axis k (staged for the owner's near box)
+    auto coordf = [&](int k, int i) -> double {
+        return cst ? s_X[k][wrap_idx(i - (sP.slo[k] - 1), a.g.n[k])] : a.coord[k][i];
+    };
     auto owner_solid = [&](int qx, int qy, int qz) -> bool {
         if (qy < sP.slo[1] || qy > sP.shi[1] || qz < sP.slo[2] || qz > sP.shi[2]) return false;
         const int r = (qy - sP.slo[1]) + ly * (qz - sP.slo[2]);
@@ -168,7 +181,7 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
     if (valid) {
         const bool oW = a.wall && a.wall[cell];
         const int tile = x / a.g.t[0] + a.g.nt[0] * (y / a.g.t[1] + a.g.nt[1] * (z / a.g.t[2]));
-        const double X0 = a.coord[0][x], X1 = a.coord[1][y], X2 = D == 3 ? a.coord[2][z] : 0.0;
+        const double X0 = coordf(0, x), X1 = coordf(1, y), X2 = D == 3 ? coordf(2, z) : 0.0;
         const double rho0 = a.rho0;
         const bool alone = is_part && s_alone;
         for (unsigned m = mask; m; m &= m - 1) {
@@ -188,7 +201,7 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
                     v += 6.0 * rhoL * dot;
                 }
                 // Ladd terms (fluids.jl:176-189) of every particle with link (x, j), in order
-                const double T0 = a.coord[0][tx], T1 = a.coord[1][ty], T2 = D == 3 ? a.coord[2][tz] : 0.0;
+                const double T0 = coordf(0, tx), T1 = coordf(1, ty), T2 = D == 3 ? coordf(2, tz) : 0.0;
                 const double wi = s_w[i];
                 int q = alone ? p : -1;
                 const ParticleDev* Pp = alone ? &sP : nullptr;
@@ -251,6 +264,11 @@ __global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
             out[k] = sum;
         }
     }
+}
+
+template <class L, int ST, bool TRT>
+__global__ void __launch_bounds__(kFixBlock) k_fixup(const StepArgs a) {
+    fixup_body<L, ST, TRT>(a, blockIdx.x);
 }
 
 }  // namespace lbm

@@ -18,7 +18,9 @@
 //      Rodrigues rotation, re-voxelisation and link-list rebuild
 //      (moveParticles!, src/gpu/particles.jl:7-92).
 // Nodes inside a particle stream like fluid, as in the reference (its
-// particle interiors are not reset).
+// particle interiors are not reset).  The three run either as separate
+// kernels in stream order or as the items of one persistent kernel per tick
+// (k_tick, tick.cuh), which overlaps the boundary work with the bulk pass.
 #pragma once
 #include <cstdint>
 #include "lattice.cuh"
@@ -52,8 +54,11 @@ struct ParticleDev {
     int kind, coupleF, coupleT, valid;
     // slip-velocity snapshot: state seen by the last getNodeVelocity call
     double sR[3], sV[3], sW[3], sE[3];
-    // mask geometry (solidRegion of the last re-voxelisation, centred at mR)
+    // mR: position at the last move (torque arm of the momentum exchange);
+    // vR: centre of the stored solid intervals, slack: min |d^2 - r^2| over the
+    // nodes of the solid box at that centre (<= 0: intervals must be rebuilt)
     double mR[3];
+    double vR[3], slack;
     int slo[3], shi[3];      // index box that contains every solid node (slo > shi: empty)
     int tlo[3], tn[3];       // tile box of the near box (periodic), for candidate bits
     unsigned dirlinks;       // bit j set: the particle has >= 1 boundary link in streaming direction j
@@ -82,7 +87,12 @@ struct StepArgs {
     const int* wnodes;                    // wall nodes (static)
     int nwlinks, nwnodes;
     int maxchunks;                        // fix-up CTAs reserved per particle
+    int vrows;                            // x-rows per tile of the vector bulk pass
+    long long vtiles;                     // tiles of the vector bulk pass
+    int vnt1;                             // vector tiles per z-slice
     int pad;
+    const int* nbox;                      // [nparts][6] solid boxes (lo, hi) the fix-up of this tick uses
+    const unsigned char* vnear;           // [vtiles] tiles next to wall links (static) or null
     double* partial;
     int* err;
     double rho0;                          // shift density of the stored populations
@@ -121,6 +131,19 @@ __device__ __forceinline__ bool sphere_test(double X0, double X1, double X2, con
         s = __dadd_rn(s, __dmul_rn(q, q));
     }
     return s < r2;
+}
+
+// the squared distance of sphere_test, same operations and rounding
+template <int D>
+__device__ __forceinline__ double sphere_d2(double X0, double X1, double X2, const double* c) {
+    double a = __dsub_rn(X0, c[0]);
+    double b = __dsub_rn(X1, c[1]);
+    double s = __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b));
+    if (D == 3) {
+        double q = __dsub_rn(X2, c[2]);
+        s = __dadd_rn(s, __dmul_rn(q, q));
+    }
+    return s;
 }
 
 // the near box of a particle: its solid box grown by one node (periodic, at
@@ -275,16 +298,24 @@ struct NodeState {
     R rho;       // rho^n
 };
 
-template <class L, int ST, bool TRT>
-__device__ __forceinline__ void load_collide(const StepArgs& a, int cell, bool valid, NodeState<L, ST, TRT>& s) {
+// the stored populations of one node, in storage units
+template <class L, int ST>
+__device__ __forceinline__ void load_pops(const StepArgs& a, int cell, bool valid, typename Store<ST>::R* g) {
     using SS = Store<ST>;
     using T = typename SS::T;
     using R = typename SS::R;
-    constexpr int Q = L::Q;
     const T* __restrict__ src = static_cast<const T*>(a.src);
     const long long N = a.g.N;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) s.g[i] = valid ? SS::dec(src[i * N + cell], R(1)) : R(0);
+    for (int i = 0; i < L::Q; ++i) g[i] = valid ? SS::dec(src[i * N + cell], R(1)) : R(0);
+}
+
+// collide loaded populations with the node's force; returns rho^n
+template <class L, int ST, bool TRT>
+__device__ __forceinline__ typename Store<ST>::R collide_node(const StepArgs& a, int cell, bool valid,
+                                                            typename Store<ST>::R* g) {
+    using R = typename Store<ST>::R;
+    const long long N = a.g.N;
     R Fx = 0, Fy = 0, Fz = 0;
     if (a.force_mode == 1) {
         Fx = R(a.F[0]);
@@ -295,7 +326,13 @@ __device__ __forceinline__ void load_collide(const StepArgs& a, int cell, bool v
         Fy = R(a.ffield[N + cell]);
         if (L::D == 3) Fz = R(a.ffield[2 * N + cell]);
     }
-    s.rho = collide<L, R, TRT>(a, s.g, Fx, Fy, Fz, a.force_mode == 2);
+    return collide<L, R, TRT>(a, g, Fx, Fy, Fz, a.force_mode == 2);
+}
+
+template <class L, int ST, bool TRT>
+__device__ __forceinline__ void load_collide(const StepArgs& a, int cell, bool valid, NodeState<L, ST, TRT>& s) {
+    load_pops<L, ST>(a, cell, valid, s.g);
+    s.rho = collide_node<L, ST, TRT>(a, cell, valid, s.g);
 }
 
 // ---------------------------------------------------------------------------
@@ -397,24 +434,26 @@ constexpr int x_slot(int i) {  // exchange slot of direction i (cx != 0)
     return n;
 }
 
-constexpr int kBlockV4 = 256;
-
-template <class L, int ST, bool TRT>
-__global__ void __launch_bounds__(kBlockV4) k_bulk_v4(const StepArgs a) {
+// One tile of the vector bulk pass: `a.vrows` full x-rows of one z-slice, four
+// consecutive x-nodes per thread with 128-bit (FP32) or 64-bit (FP16/BF16)
+// loads and stores.  Because a CTA owns whole x-rows, the periodic x-wrap
+// stays inside the CTA: pushes along +-x are realigned in registers, the one
+// value per row segment that crosses into the neighbouring thread goes
+// through shared memory, and every global store is an aligned vector store.
+// Threads past the tile's rows only take part in the barrier.
+template <class L, int ST, bool TRT, int B>
+__device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, float (*s_ex)[B]) {
     using R = float;
     constexpr int Q = L::Q;
-    constexpr int NXD = x_moving_dirs<L>();
-    __shared__ R s_ex[NXD][kBlockV4];
-    const long long tile = blockIdx.x;
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
     const int RT = nx >> 2;  // threads per x-row
     const int tid = threadIdx.x;
     const int row = tid / RT, j = tid - row * RT;
-    const int by = (int)(tile % a.g.nt[1]);
-    const int bz = (int)(tile / a.g.nt[1]);
-    const int y = by * a.g.t[1] + row;
+    const int by = (int)(tile % a.vnt1);
+    const int bz = (int)(tile / a.vnt1);
+    const int y = by * a.vrows + row;
     const int z = bz;
-    const bool valid = y < ny;
+    const bool valid = row < a.vrows && y < ny;
     const int x0 = 4 * j;
     const int cell0 = valid ? x0 + nx * (y + ny * z) : 0;
     R g[4][Q];
@@ -431,10 +470,12 @@ __global__ void __launch_bounds__(kBlockV4) k_bulk_v4(const StepArgs a) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) collide<L, R, TRT>(a, g[k], Fx, Fy, Fz, false);
     // the value of each +-x direction that leaves this thread's 4-node segment
+    if (row < a.vrows) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        if (L::cx(i) == 1) s_ex[x_slot<L>(i)][tid] = g[3][i];
-        if (L::cx(i) == -1) s_ex[x_slot<L>(i)][tid] = g[0][i];
+        for (int i = 0; i < Q; ++i) {
+            if (L::cx(i) == 1) s_ex[x_slot<L>(i)][tid] = g[3][i];
+            if (L::cx(i) == -1) s_ex[x_slot<L>(i)][tid] = g[0][i];
+        }
     }
     __syncthreads();
     if (!valid) return;
@@ -453,6 +494,33 @@ __global__ void __launch_bounds__(kBlockV4) k_bulk_v4(const StepArgs a) {
             Vec4<ST>::store(a.dstq[i], t0, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right]);
         }
     }
+}
+
+// the vector bulk pass over all tiles, one CTA of B threads per tile.
+// Registers are capped at 128 per thread (512 / B resident CTAs).
+template <class L, int ST, bool TRT, int B>
+__global__ void __launch_bounds__(B, 512 / B) k_bulk_v4(const StepArgs a) {
+    __shared__ float s_ex[x_moving_dirs<L>()][B];
+    bulk_v4_tile<L, ST, TRT, B>(a, blockIdx.x, s_ex);
+}
+
+// periodic intervals [a0, a0+la) and [b0, b0+lb) of an axis of n nodes meet
+__device__ __forceinline__ bool ranges_meet(int a0, int la, int b0, int lb, int n) {
+    if (la >= n || lb >= n) return true;
+    const int d = ((b0 - a0) % n + n) % n;  // start of b relative to a
+    return d < la || d + lb > n;
+}
+
+// does vector tile `tile` come within two nodes of particle p's solid box?
+template <int D>
+__device__ __forceinline__ bool tile_meets_box(const StepArgs& a, long long tile, int p) {
+    const int by = (int)(tile % a.vnt1), bz = (int)(tile / a.vnt1);
+    const int ny = a.g.n[1], nz = a.g.n[2];
+    const int y0 = by * a.vrows, ly = min(a.vrows, ny - y0);
+    const int* b = a.nbox + 6 * p;
+    if (b[0] > b[3] || b[1] > b[4] || b[2] > b[5]) return false;  // no solid node
+    if (!ranges_meet(y0, ly, b[1] - 2, b[4] - b[1] + 5, ny)) return false;
+    return D == 2 || ranges_meet(bz, 1, b[2] - 2, b[5] - b[2] + 5, nz);
 }
 
 }  // namespace lbm

@@ -3,8 +3,9 @@
 // Host side of the drop-in boundary: validates the resolved modelInit /
 // addSquirmer! keyword sets, owns all device memory of a model, and runs
 // LBMpropagate! as CUDA-graph replays of the tick
-//     k_bulk(_v4) -> k_fixup -> k_particles
-// on one stream.
+//     k_tick (one persistent kernel: bulk, fix-up and particle update items)
+// or, where it does not apply, k_bulk(_v4) -> k_fixup on the main stream with
+// k_particles on a side stream (see enqueue_tick).
 #include "lbm_b200.h"
 #include "ops.cuh"
 
@@ -38,6 +39,7 @@ struct lbm_handle {
     // configuration
     int device = 0;
     int dims = 0, q = 0, lattice = 0, storage = 0, trt = 0;
+    int schedule = 0;  // LBM_SCHEDULE_* (resolved: never AUTO)
     int n[3] = {1, 1, 1};
     long long N = 0;
     GridDesc g{};
@@ -54,6 +56,21 @@ struct lbm_handle {
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev_fix = nullptr, ev_part = nullptr;
     bool part_pending = false;
+    // vector bulk pass: tiles of vrows full x-rows, vblock threads per tile
+    int vrows = 0, vnt1 = 0, vblock = 0;
+    long long vtiles = 0;
+    std::vector<unsigned char> vnear;  // static near flags of the tiles (walls)
+    unsigned char* d_vnear = nullptr;
+    int* d_nbox[2] = {nullptr, nullptr};  // published solid boxes, [pcap][6] each
+    // persistent tick kernel: item maps, per-parity arguments, queue counters
+    bool tick_ready = false;
+    unsigned tick_grid = 0;
+    TickItems items{};
+    int4* d_amap = nullptr;
+    int2 *d_bmap = nullptr, *d_cmap = nullptr, *d_dmap = nullptr;
+    StepArgs* d_targs = nullptr;      // [2]: by source buffer
+    ParticleArgs* d_pargs = nullptr;  // [2]
+    TickCounters* d_tq = nullptr;
     void* pop[2] = {nullptr, nullptr};
     int cur = 0;
     double* d_coord[3] = {nullptr, nullptr, nullptr};
@@ -200,6 +217,7 @@ int ensure_tmp(lbm_handle* h, size_t bytes) {
 }
 
 void drop_graphs(lbm_handle* h) {
+    h->tick_ready = false;  // the tick kernel's maps and arguments are rebuilt with the graphs
     for (auto& row : h->graphs)
         for (auto& gr : row) {
             if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -227,6 +245,11 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.nwlinks = h->nwlinks;
     a.nwnodes = h->nwnodes;
     a.maxchunks = h->maxchunks;
+    a.vrows = h->vrows;
+    a.vnt1 = h->vnt1;
+    a.vtiles = h->vtiles;
+    a.nbox = h->d_nbox[src];
+    a.vnear = h->d_vnear;
     a.partial = h->d_partial;
     a.err = h->d_err;
     a.rho0 = h->rho0;
@@ -269,12 +292,23 @@ StepArgs step_args(const lbm_handle* h, int src) {
 }
 
 bool use_vector_bulk(const lbm_handle* h) {
-    return h->ops.bulk_v4 != nullptr && h->force_mode != LBM_FORCE_FIELD && h->n[0] % 4 == 0 &&
-           h->g.t[0] == h->n[0] && (h->n[0] / 4) * h->g.t[1] <= kBlockV4;
+    return h->ops.bulk_v4 != nullptr && h->force_mode != LBM_FORCE_FIELD && h->vrows > 0;
 }
 
-ParticleArgs particle_args(const lbm_handle* h, int mode, int pid) {
+// the bulk pass over all tiles
+void launch_bulk(const lbm_handle* h, const StepArgs& a, cudaStream_t s) {
+    if (use_vector_bulk(h))
+        h->ops.bulk_v4(a, h->vtiles, h->vblock, s);
+    else
+        h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), s);
+}
+
+// `src`: population buffer of the tick (selects the published-box buffer);
+// -1 publishes into both (setup)
+ParticleArgs particle_args(const lbm_handle* h, int mode, int pid, int src = -1) {
     ParticleArgs a{};
+    a.nbox_out[0] = src < 0 ? h->d_nbox[0] : h->d_nbox[src];
+    a.nbox_out[1] = src < 0 ? h->d_nbox[1] : nullptr;
     a.parts = h->d_parts;
     a.nparts = (int)h->hparts.size();
     a.mode = mode;
@@ -315,8 +349,76 @@ long long fixup_blocks(const lbm_handle* h) {
            (h->nwnodes + kFixBlock - 1) / kFixBlock;
 }
 
+// the persistent tick kernel applies to the vector bulk kernel with
+// kTickBlock-thread tiles, when there is boundary work to overlap
+bool use_tick_kernel(const lbm_handle* h) {
+    return h->schedule == LBM_SCHEDULE_PERSISTENT && use_vector_bulk(h) && h->ops.tick != nullptr &&
+           h->vblock == kTickBlock && h->tick_grid > 0 && fixup_blocks(h) > 0;
+}
+
+// (Re)build the item maps and the per-parity arguments of the tick kernel.
+int prepare_tick(lbm_handle* h) {
+    if (h->tick_ready || !use_tick_kernel(h)) return LBM_OK;
+    const int np = (int)h->hparts.size();
+    std::vector<int4> am;
+    for (long long t = 0; t < (long long)h->vnear.size(); ++t)
+        if (h->vnear[t]) am.push_back(make_int4(0, 0, (int)t, 0));
+    for (int p = 0; p < np; ++p) {
+        // a solid box spans at most 2r/dx + 5 nodes per axis; grown by two on each side
+        const long long len = (long long)std::floor(2.0 * h->hparts[p].radius / h->dx) + 9;
+        const long long nys = std::min<long long>(h->vnt1 + 1, (len + h->vrows - 1) / h->vrows + 2);
+        const long long nzs = h->dims == 3 ? std::min<long long>(h->n[2], len) : 1;
+        if (nys >= 65536 || nzs >= 32768)
+            return set_err(h, LBM_ERR_UNSUPPORTED, "particle too large for the tick kernel's tile slots");
+        for (long long dz = 0; dz < nzs; ++dz)
+            for (long long dy = 0; dy < nys; ++dy) am.push_back(make_int4(0, 1, p, (int)(dy | (dz << 16))));
+    }
+    std::vector<int2> bm, cm, dm;
+    const long long nb = fixup_blocks(h);
+    for (long long b = 0; b < nb; ++b) bm.push_back(make_int2(0, (int)b));
+    for (int p = 0; p < np; ++p) cm.push_back(make_int2(0, p));
+    for (long long t = 0; t < h->vtiles; ++t) dm.push_back(make_int2(0, (int)t));
+    StepArgs ta[2];
+    ParticleArgs pa[2];
+    for (int s = 0; s < 2; ++s) {
+        ta[s] = step_args(h, s);
+        ta[s].nbox = h->d_nbox[1 - s];  // boxes of the previous tick's update (see tick.cuh)
+        pa[s] = particle_args(h, 0, 0, s);
+    }
+    dev_free(h->d_amap);
+    dev_free(h->d_bmap);
+    dev_free(h->d_cmap);
+    dev_free(h->d_dmap);
+    int rc = dev_alloc(h, &h->d_amap, sizeof(int4) * std::max<size_t>(1, am.size()));
+    if (!rc) rc = dev_alloc(h, &h->d_bmap, sizeof(int2) * std::max<size_t>(1, bm.size()));
+    if (!rc) rc = dev_alloc(h, &h->d_cmap, sizeof(int2) * std::max<size_t>(1, cm.size()));
+    if (!rc) rc = dev_alloc(h, &h->d_dmap, sizeof(int2) * std::max<size_t>(1, dm.size()));
+    if (!rc && !h->d_targs) rc = dev_alloc(h, &h->d_targs, sizeof(StepArgs) * 2);
+    if (!rc && !h->d_pargs) rc = dev_alloc(h, &h->d_pargs, sizeof(ParticleArgs) * 2);
+    if (rc) return rc;
+    if (!am.empty()) CUDA_TRY(h, cudaMemcpyAsync(h->d_amap, am.data(), sizeof(int4) * am.size(), cudaMemcpyHostToDevice, h->stream));
+    if (!bm.empty()) CUDA_TRY(h, cudaMemcpyAsync(h->d_bmap, bm.data(), sizeof(int2) * bm.size(), cudaMemcpyHostToDevice, h->stream));
+    if (!cm.empty()) CUDA_TRY(h, cudaMemcpyAsync(h->d_cmap, cm.data(), sizeof(int2) * cm.size(), cudaMemcpyHostToDevice, h->stream));
+    if (!dm.empty()) CUDA_TRY(h, cudaMemcpyAsync(h->d_dmap, dm.data(), sizeof(int2) * dm.size(), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_targs, ta, sizeof(ta), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_pargs, pa, sizeof(pa), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->items.amap = h->d_amap;
+    h->items.bmap = h->d_bmap;
+    h->items.cmap = h->d_cmap;
+    h->items.dmap = h->d_dmap;
+    h->items.na = (long long)am.size();
+    h->items.nb = (long long)bm.size();
+    h->items.nc = (long long)cm.size();
+    h->items.nd = (long long)dm.size();
+    h->tick_ready = true;
+    return LBM_OK;
+}
+
 int launches_per_tick(const lbm_handle* h) {
-    return 1 + (fixup_blocks(h) > 0 ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
+    if (use_tick_kernel(h)) return 1;
+    const bool fix = fixup_blocks(h) > 0;
+    return 1 + (fix ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
 }
 
 // events of graph slot s: [0] before bulk, [1] after bulk, [2] after fix-up, [3] after particles
@@ -334,17 +436,20 @@ void prof_record(lbm_handle* h, int slot, int k, cudaStream_t s) {
 }
 
 // Enqueue one tick (capturable); `slot` selects the profiling events.
-// Stream order:  main: bulk(n) -> [wait particles(n-1)] -> fixup(n) -> bulk(n+1) ...
-//                side:                    particles(n) after fixup(n)
+// Persistent tick kernel: one launch.  Otherwise
+//   main: bulk(n) -> [wait particles(n-1)] -> fixup(n) -> bulk(n+1) ...
+//   side:                    particles(n) after fixup(n)
 // The bulk pass never reads particle state, so the particle update of tick n
 // runs concurrently with the bulk pass of tick n+1.
 void enqueue_tick(lbm_handle* h, int src, int slot) {
-    const StepArgs a = step_args(h, src);
     prof_record(h, slot, 0, h->stream);
-    if (use_vector_bulk(h))
-        h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
-    else
-        h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+    if (use_tick_kernel(h)) {
+        h->ops.tick(h->d_targs + src, h->d_pargs + src, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
+        prof_record(h, slot, 1, h->stream);
+        return;
+    }
+    const StepArgs a = step_args(h, src);
+    launch_bulk(h, a, h->stream);
     prof_record(h, slot, 1, h->stream);
     if (h->part_pending) {
         cudaStreamWaitEvent(h->stream, h->ev_part, 0);
@@ -357,14 +462,14 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
         cudaEventRecord(h->ev_fix, h->stream);
         cudaStreamWaitEvent(h->side, h->ev_fix, 0);
         prof_record(h, slot, 2, h->side);
-        h->ops.particles(particle_args(h, 0, 0), (unsigned)a.nparts, h->side);
+        h->ops.particles(particle_args(h, 0, 0, src), (unsigned)a.nparts, h->side);
         prof_record(h, slot, 3, h->side);
         cudaEventRecord(h->ev_part, h->side);
         h->part_pending = true;
     }
 }
 
-// make the main stream wait for an outstanding particle update
+// make the main stream wait for outstanding side-stream work
 void join_particles(lbm_handle* h) {
     if (h->part_pending) {
         cudaStreamWaitEvent(h->stream, h->ev_part, 0);
@@ -403,6 +508,7 @@ int check_device_error(lbm_handle* h) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (err & kErrLinkOverflow) return set_err(h, LBM_ERR_STATE, "particle boundary links exceeded their capacity");
     if (err & kErrIntervalOverflow) return set_err(h, LBM_ERR_STATE, "particle solid box exceeded its capacity");
+    if (err & kErrSpinTimeout) return set_err(h, LBM_ERR_TIMEOUT, "a wait inside the tick kernel gave up");
     return LBM_OK;
 }
 
@@ -418,6 +524,28 @@ void choose_tiles(lbm_handle* h) {
     for (int k = 0; k < 3; ++k) g.nt[k] = (h->n[k] + g.t[k] - 1) / g.t[k];
     g.N = h->N;
     g.ntiles = (long long)g.nt[0] * g.nt[1] * g.nt[2];
+    // vector tiles: whole x-rows, 4 nodes per thread.  Rows of up to 256
+    // nodes take kTickBlock-thread CTAs (the persistent tick kernel's size);
+    // wider rows the CTA size (up to 512) that leaves the fewest idle threads.
+    h->vrows = h->vnt1 = h->vblock = 0;
+    h->vtiles = 0;
+    if (h->n[0] % 4 == 0 && h->n[0] / 4 <= 512) {
+        const int RT = h->n[0] / 4;
+        double best = -1.0;
+        for (int B : kBulkBlocks) {
+            if (B < RT) continue;
+            const int rows = std::min(B / RT, h->n[1]);
+            const double use = (double)(rows * RT) / B;
+            if (use > best + 1e-9) {
+                best = use;
+                h->vblock = B;
+            }
+        }
+        if (RT <= kTickBlock) h->vblock = kTickBlock;
+        h->vrows = std::max(1, std::min(h->vblock / RT, h->n[1]));
+        h->vnt1 = (h->n[1] + h->vrows - 1) / h->vrows;
+        h->vtiles = (long long)h->vnt1 * h->n[2];
+    }
 }
 
 int upload(lbm_handle* h, void* dst, const void* src, size_t bytes) {
@@ -445,6 +573,16 @@ void destroy_all(lbm_handle* h) {
     dev_free(h->d_partial);
     dev_free(h->d_err);
     dev_free(h->d_tmp);
+    dev_free(h->d_vnear);
+    dev_free(h->d_nbox[0]);
+    dev_free(h->d_nbox[1]);
+    dev_free(h->d_amap);
+    dev_free(h->d_bmap);
+    dev_free(h->d_cmap);
+    dev_free(h->d_dmap);
+    dev_free(h->d_targs);
+    dev_free(h->d_pargs);
+    dev_free(h->d_tq);
     for (auto& e : h->pev) cudaEventDestroy(e);
     if (h->t_begin) cudaEventDestroy(h->t_begin);
     if (h->t_end) cudaEventDestroy(h->t_end);
@@ -484,9 +622,21 @@ int ensure_particle_capacity(lbm_handle* h, int nparts_new) {
         if (h->d_parts && !h->hparts.empty())
             CUDA_TRY(h, cudaMemcpyAsync(np, h->d_parts, sizeof(ParticleDev) * h->hparts.size(),
                                         cudaMemcpyDeviceToDevice, h->stream));
+        int* nb[2] = {nullptr, nullptr};
+        for (int b = 0; b < 2; ++b) {
+            rc = dev_alloc(h, &nb[b], sizeof(int) * 6 * cap);
+            if (rc) return rc;
+            if (h->d_nbox[b] && !h->hparts.empty())
+                CUDA_TRY(h, cudaMemcpyAsync(nb[b], h->d_nbox[b], sizeof(int) * 6 * h->hparts.size(),
+                                            cudaMemcpyDeviceToDevice, h->stream));
+        }
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         dev_free(h->d_parts);
         h->d_parts = np;
+        for (int b = 0; b < 2; ++b) {
+            dev_free(h->d_nbox[b]);
+            h->d_nbox[b] = nb[b];
+        }
         h->pcap = cap;
     }
     const int words_new = std::max(1, (nparts_new + 63) / 64);
@@ -589,6 +739,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         N *= na;
     }
     if (N >= (1LL << 31)) return set_err(nullptr, LBM_ERR_UNSUPPORTED, "more than 2^31 lattice nodes");
+    if (cfg->schedule < LBM_SCHEDULE_AUTO || cfg->schedule > LBM_SCHEDULE_PERSISTENT || cfg->schedule == 2)
+        return set_err(nullptr, LBM_ERR_INVALID, "unknown schedule");
     if (cfg->force_mode < LBM_FORCE_NONE || cfg->force_mode > LBM_FORCE_FIELD)
         return set_err(nullptr, LBM_ERR_INVALID, "unknown force mode");
     if (cfg->force_mode == LBM_FORCE_FIELD && !cfg->force_field)
@@ -614,6 +766,7 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
                    ? (cfg->store_scale > 0 ? cfg->store_scale : 4096.0)
                    : 1.0;
     h->force_mode = cfg->force_mode;
+    h->schedule = cfg->schedule == LBM_SCHEDULE_AUTO ? LBM_SCHEDULE_STREAM : cfg->schedule;
     if (cfg->force_mode == LBM_FORCE_UNIFORM)
         for (int k = 0; k < cfg->dims; ++k) h->F[k] = cfg->force[k];
     h->incompressible = cfg->compressible ? 0 : 1;
@@ -632,6 +785,10 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         }
     }
     choose_tiles(h);
+    if (!h->ops.bulk_v4 || h->force_mode == LBM_FORCE_FIELD) {  // scalar bulk kernel
+        h->vrows = h->vnt1 = h->vblock = 0;
+        h->vtiles = 0;
+    }
     int rc = LBM_OK;
 #define TRY(x)                       \
     do {                             \
@@ -644,11 +801,25 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
     } while (0)
     TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess
             ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
-    TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) == cudaSuccess
-            ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
+    {  // the side stream (fix-up, particle update) takes SM slots ahead of the bulk pass
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        TRY(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi) == cudaSuccess
+                ? LBM_OK : set_err(h, LBM_ERR_CUDA, "stream creation failed"));
+    }
     TRY(cudaEventCreateWithFlags(&h->ev_fix, cudaEventDisableTiming) == cudaSuccess &&
                 cudaEventCreateWithFlags(&h->ev_part, cudaEventDisableTiming) == cudaSuccess
             ? LBM_OK : set_err(h, LBM_ERR_CUDA, "event creation failed"));
+    TRY(dev_alloc(h, &h->d_tq, sizeof(TickCounters)));
+    if (cudaMemsetAsync(h->d_tq, 0, sizeof(TickCounters), h->stream) != cudaSuccess)
+        TRY(set_err(h, LBM_ERR_CUDA, "memset failed"));
+    if (h->vtiles > 0 && h->vblock == kTickBlock && h->ops.tick_fn) {  // persistent grid: all resident CTAs
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h->ops.tick_fn, kTickBlock, 0) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+            TRY(set_err(h, LBM_ERR_CUDA, "occupancy query failed"));
+        h->tick_grid = (unsigned)std::max(0, per_sm * sms);
+    }
     const size_t pop_bytes = (size_t)N * h->q * storage_bytes(h->storage);
     TRY(dev_alloc(h, &h->pop[0], pop_bytes));
     TRY(dev_alloc(h, &h->pop[1], pop_bytes));
@@ -685,6 +856,24 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         TRY(dev_alloc(h, &h->d_wnodes, sizeof(int) * std::max<size_t>(1, wn.size())));
         if (!wl.empty()) TRY(upload(h, h->d_wlinks, wl.data(), sizeof(int2) * wl.size()));
         if (!wn.empty()) TRY(upload(h, h->d_wnodes, wn.data(), sizeof(int) * wn.size()));
+        if (h->vtiles > 0) {  // vector tiles within one node of a wall node or wall link
+            std::vector<unsigned char>& vn = h->vnear;
+            vn.assign(h->vtiles, 0);
+            auto mark = [&](long long c) {
+                const int y = (int)((c / h->n[0]) % h->n[1]), z = (int)(c / ((long long)h->n[0] * h->n[1]));
+                for (int dz = -1; dz <= 1; ++dz) {
+                    if (h->dims == 2 && dz != 0) continue;
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const int yy = (y + dy + h->n[1]) % h->n[1], zz = (z + dz + h->n[2]) % h->n[2];
+                        vn[yy / h->vrows + (long long)h->vnt1 * zz] = 1;
+                    }
+                }
+            };
+            for (const int2& e : wl) mark(e.x);
+            for (int c : wn) mark(c);
+            TRY(dev_alloc(h, &h->d_vnear, h->vtiles));
+            TRY(upload(h, h->d_vnear, vn.data(), h->vtiles));
+        }
         if (cudaStreamSynchronize(h->stream) != cudaSuccess) TRY(set_err(h, LBM_ERR_CUDA, "upload failed"));
     }
     TRY(ensure_particle_capacity(h, 0));
@@ -851,6 +1040,10 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
     if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
     if (nsteps < 0) return set_err(h, LBM_ERR_INVALID, "ticks must be non-negative");
     BIND(h);
+    {
+        const int rc = prepare_tick(h);
+        if (rc) return rc;
+    }
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_begin, h->stream));
     int64_t done = 0;
     int slots_used = 0;
@@ -881,7 +1074,8 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
         float ms = 0;
         CUDA_TRY(h, cudaEventElapsedTime(&ms, h->t_begin, h->t_end));
         p.total_ms = ms;
-        const bool fix = fixup_blocks(h) > 0;
+        const bool fused = use_tick_kernel(h);  // one kernel: its time is reported as bulk_ms
+        const bool fix = !fused && fixup_blocks(h) > 0;
         double sb = 0, sf = 0, sp = 0;
         if (h->profiling < 2) slots_used = 0;  // per-kernel events were not recorded
         for (int s = 0; s < slots_used; ++s) {
@@ -891,7 +1085,7 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
                 CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 1), prof_event(h, s, 2)));
                 sf += ms;
             }
-            if (!h->hparts.empty()) {
+            if (!fused && !h->hparts.empty()) {
                 CUDA_TRY(h, cudaEventElapsedTime(&ms, prof_event(h, s, 2), prof_event(h, s, 3)));
                 sp += ms;
             }
@@ -932,23 +1126,30 @@ int lbm_get_profile(lbm_handle* h, lbm_profile* out) {
 
 int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg_ms) {
     if (!h || !avg_ms) return set_err(h, LBM_ERR_INVALID, "null argument");
-    if (kernel < LBM_KERNEL_BULK || kernel > LBM_KERNEL_PARTICLES || launches < 1)
+    if (kernel < LBM_KERNEL_BULK || kernel > LBM_KERNEL_TICK || launches < 1)
         return set_err(h, LBM_ERR_INVALID, "unknown kernel or launch count");
     BIND(h);
     const int np = (int)h->hparts.size();
     if (kernel == LBM_KERNEL_FIXUP && fixup_blocks(h) == 0) return set_err(h, LBM_ERR_STATE, "model has no boundary links");
     if (kernel == LBM_KERNEL_PARTICLES && np == 0) return set_err(h, LBM_ERR_STATE, "model has no particles");
+    if (kernel == LBM_KERNEL_TICK) {
+        if (!use_tick_kernel(h)) return set_err(h, LBM_ERR_STATE, "the persistent tick kernel does not apply");
+        const int rc0 = prepare_tick(h);
+        if (rc0) return rc0;
+    }
     // save everything the launches touch
     const size_t pop_bytes = (size_t)h->N * h->q * storage_bytes(h->storage);
     const size_t parts_b = sizeof(ParticleDev) * np, ivl_b = sizeof(int2) * h->ivl_slots,
-                 link_b = sizeof(int2) * h->link_slots, bits_b = sizeof(unsigned long long) * h->g.ntiles * h->words;
+                 link_b = sizeof(int2) * h->link_slots, bits_b = sizeof(unsigned long long) * h->g.ntiles * h->words,
+                 box_b = sizeof(int) * 6 * np;
+    const size_t save_b = 2 * pop_bytes + parts_b + ivl_b + link_b + bits_b + 2 * box_b;
     char* save = nullptr;
-    int rc = dev_alloc(h, &save, 2 * pop_bytes + parts_b + ivl_b + link_b + bits_b);
+    int rc = dev_alloc(h, &save, save_b);
     if (rc) return rc;
     char* sp = save;
-    const void* srcs[6] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits};
-    const size_t sizes[6] = {pop_bytes, pop_bytes, parts_b, ivl_b, link_b, bits_b};
-    for (int k = 0; k < 6; ++k) {
+    const void* srcs[8] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits, h->d_nbox[0], h->d_nbox[1]};
+    const size_t sizes[8] = {pop_bytes, pop_bytes, parts_b, ivl_b, link_b, bits_b, box_b, box_b};
+    for (int k = 0; k < 8; ++k) {
         if (sizes[k] && srcs[k]) CUDA_TRY(h, cudaMemcpyAsync(sp, srcs[k], sizes[k], cudaMemcpyDeviceToDevice, h->stream));
         sp += sizes[k];
     }
@@ -960,15 +1161,15 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
     for (int l = 0; l < launches; ++l) {
         const StepArgs a = step_args(h, b);
         if (kernel == LBM_KERNEL_BULK) {
-            if (use_vector_bulk(h))
-                h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
-            else
-                h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+            launch_bulk(h, a, h->stream);
             b = 1 - b;
         } else if (kernel == LBM_KERNEL_FIXUP) {
             h->ops.fixup(a, (unsigned)fixup_blocks(h), h->stream);
+        } else if (kernel == LBM_KERNEL_TICK) {
+            h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
+            b = 1 - b;
         } else {
-            h->ops.particles(particle_args(h, 0, 0), (unsigned)np, h->stream);
+            h->ops.particles(particle_args(h, 0, 0, b), (unsigned)np, h->stream);
         }
     }
     CUDA_TRY(h, cudaEventRecord(e1, h->stream));
@@ -980,14 +1181,14 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
     cudaEventDestroy(e1);
     *avg_ms = ms / launches;
     sp = save;
-    void* dsts[6] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits};
-    for (int k = 0; k < 6; ++k) {
+    void* dsts[8] = {h->pop[0], h->pop[1], h->d_parts, h->d_ivl, h->d_links, h->d_tilebits, h->d_nbox[0], h->d_nbox[1]};
+    for (int k = 0; k < 8; ++k) {
         if (sizes[k] && dsts[k]) CUDA_TRY(h, cudaMemcpyAsync(dsts[k], sp, sizes[k], cudaMemcpyDeviceToDevice, h->stream));
         sp += sizes[k];
     }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     dev_free(save);
-    h->device_bytes -= 2 * pop_bytes + parts_b + ivl_b + link_b + bits_b;
+    h->device_bytes -= save_b;
     return check_device_error(h);
 }
 
@@ -1309,6 +1510,11 @@ StepArgs noalloc_step_args(const lbm_handle* h, int src, double* partial) {
     a.nwlinks = h->nwlinks;
     a.nwnodes = h->nwnodes;
     a.maxchunks = h->maxchunks;
+    a.vrows = h->vrows;
+    a.vnt1 = h->vnt1;
+    a.vtiles = h->vtiles;
+    a.nbox = h->d_nbox[src];
+    a.vnear = h->d_vnear;
     a.partial = partial;
     a.err = h->d_err;
     a.rho0 = h->rho0;
@@ -1373,16 +1579,14 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
     if (rc) return rc;
     if (slots > 0)  // slots used by this model start from zero in every call
         CUDA_TRY(h, cudaMemsetAsync(scratch, 0, sizeof(double) * kPartialStride * slots, h->stream));
-    ParticleArgs pa = particle_args(h, 0, 0);
+    ParticleArgs pa = particle_args(h, 0, 0, h->cur);
     pa.partial = scratch;
     const long long nb = fixup_blocks(h);
     const int np = (int)h->hparts.size();
     for (int64_t s = 0; s < nsteps; ++s) {
         const StepArgs a = noalloc_step_args(h, h->cur, scratch);
-        if (use_vector_bulk(h))
-            h->ops.bulk_v4(a, (unsigned)h->g.ntiles, dim3((h->n[0] / 4) * h->g.t[1]), h->stream);
-        else
-            h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), h->stream);
+        pa.nbox_out[0] = h->d_nbox[h->cur];
+        launch_bulk(h, a, h->stream);
         if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
         if (np > 0) h->ops.particles(pa, (unsigned)np, h->stream);
         h->cur = 1 - h->cur;

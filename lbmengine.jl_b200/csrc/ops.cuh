@@ -5,12 +5,12 @@
 #include "fixup.cuh"
 #include "particles.cuh"
 #include "aux_kernels.cuh"
+#include "tick.cuh"
 
 namespace lbm {
 
 struct Ops {
     void (*bulk)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
-    void (*bulk_v4)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);  // null: not instantiated
     void (*fixup)(const StepArgs&, unsigned grid, cudaStream_t);
     void (*particles)(const ParticleArgs&, unsigned grid, cudaStream_t);
     void (*encode)(const CodecArgs&, cudaStream_t);
@@ -19,9 +19,17 @@ struct Ops {
     void (*check)(const CodecArgs&, int*, cudaStream_t);
     void (*init)(const InitArgs&, cudaStream_t);
     void (*mask)(const MaskArgs&, cudaStream_t);
+    // vector bulk pass over all tiles, CTAs of `block` threads (64..512); null for FP64
+    void (*bulk_v4)(const StepArgs&, long long tiles, int block, cudaStream_t);
+    // one persistent kernel per tick over the A/B/C/D item queue (tick.cuh)
+    void (*tick)(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
+                 int* err, unsigned grid, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
     const void* fixup_fn;
+    const void* tick_fn;
 };
+
+constexpr int kBulkBlocks[4] = {64, 128, 256, 512};  // CTA sizes of the vector bulk kernel
 
 inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
@@ -30,14 +38,24 @@ struct OpsImpl {
     static void bulk(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
         k_bulk<L, ST, TRT><<<grid, block, 0, s>>>(a);
     }
-    static void bulk_v4(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
-        if constexpr (ST != ST_F64) k_bulk_v4<L, ST, TRT><<<grid, block, 0, s>>>(a);
-    }
     static void fixup(const StepArgs& a, unsigned grid, cudaStream_t s) {
         k_fixup<L, ST, TRT><<<grid, kFixBlock, 0, s>>>(a);
     }
     static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
-        k_particles<L><<<grid, 256, 0, s>>>(a);
+        k_particles<L><<<grid, kPartBlock, 0, s>>>(a);
+    }
+    static void bulk_v4(const StepArgs& a, long long tiles, int block, cudaStream_t s) {
+        if constexpr (ST != ST_F64) {
+            const unsigned g = (unsigned)tiles;
+            if (block <= 64) k_bulk_v4<L, ST, TRT, 64><<<g, 64, 0, s>>>(a);
+            else if (block <= 128) k_bulk_v4<L, ST, TRT, 128><<<g, 128, 0, s>>>(a);
+            else if (block <= 256) k_bulk_v4<L, ST, TRT, 256><<<g, 256, 0, s>>>(a);
+            else k_bulk_v4<L, ST, TRT, 512><<<g, 512, 0, s>>>(a);
+        }
+    }
+    static void tick(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
+                     int* err, unsigned grid, cudaStream_t s) {
+        if constexpr (ST != ST_F64) k_tick<L, ST, TRT><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
     }
     static void encode(const CodecArgs& a, cudaStream_t s) { k_encode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
@@ -50,7 +68,6 @@ struct OpsImpl {
     static Ops make() {
         Ops o;
         o.bulk = bulk;
-        o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
         o.fixup = fixup;
         o.particles = particles;
         o.encode = encode;
@@ -59,8 +76,12 @@ struct OpsImpl {
         o.check = check;
         o.init = init;
         o.mask = mask;
+        o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
+        o.tick = ST == ST_F64 ? nullptr : tick;
         o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
         o.fixup_fn = (const void*)k_fixup<L, ST, TRT>;
+        o.tick_fn = nullptr;
+        if constexpr (ST != ST_F64) o.tick_fn = (const void*)k_tick<L, ST, TRT>;
         return o;
     }
 };

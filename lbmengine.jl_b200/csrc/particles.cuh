@@ -14,7 +14,8 @@
 
 namespace lbm {
 
-constexpr int kIvlSmem = 2048;  // rows of solid intervals staged in shared memory
+constexpr int kIvlSmem = 512;  // rows of solid intervals staged in shared memory
+constexpr int kPartBlock = 256;  // CTA size of the stand-alone particle kernel
 
 struct ParticleArgs {
     ParticleDev* parts;
@@ -32,7 +33,20 @@ struct ParticleArgs {
     double x0[3];
     double dx, dt;
     int* err;
+    int* nbox_out[2];  // [nparts][6] solid boxes (lo, hi) published for the bulk pass two ticks
+                       // later (tick update writes [0]; setup writes both); null to skip
 };
+
+// publish particle p's solid box for the far/near split of the bulk pass
+__device__ __forceinline__ void publish_box(const ParticleArgs& a, int p, const ParticleDev& P) {
+    for (int b = 0; b < 2; ++b) {
+        if (!a.nbox_out[b]) continue;
+        for (int k = 0; k < 3; ++k) {
+            a.nbox_out[b][6 * p + k] = P.slo[k];
+            a.nbox_out[b][6 * p + 3 + k] = P.shi[k];
+        }
+    }
+}
 
 // index box (clipped, not periodic) that contains every node of the sphere;
 // the +-1 margin absorbs the rounding of the affine index estimate
@@ -89,7 +103,7 @@ __device__ __forceinline__ void tile_bits_update(const ParticleArgs& a, const in
     }
 }
 
-// exclusive prefix sum of one flag per thread over the CTA (256 threads)
+// exclusive prefix sum of one flag per thread over the CTA (at most 256 threads)
 __device__ __forceinline__ int block_scan(int flag, int* s_warp, int* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int v = flag;
@@ -116,12 +130,12 @@ __device__ __forceinline__ int block_scan(int flag, int* s_warp, int* total) {
 }
 
 template <class L>
-__global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
+__device__ __forceinline__ void particles_body(const ParticleArgs& a, const int p) {
     constexpr int D = L::D;
-    const int p = a.mode != 0 ? a.setup_pid : (int)blockIdx.x;
     const int tid = threadIdx.x;
     __shared__ double s_red[8][6];
-    __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty;
+    __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty, s_keep;
+    __shared__ unsigned long long s_slack;  // bit pattern of a non-negative double
     __shared__ unsigned s_links;
     __shared__ int s_warp[9];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
@@ -233,12 +247,41 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
         s_changed = (a.mode != 0 || !P.valid) ? 1 : 0;
         s_bad = 0;
         s_nonempty = 0;
+        s_slack = (unsigned long long)__double_as_longlong(1e300);
         for (int k = 0; k < 3; ++k) {
             s_oldbox[k] = P.tlo[k];
             s_oldbox[3 + k] = P.valid ? P.tn[k] : 0;
         }
+        s_keep = 0;
         if (moved) {
             for (int k = 0; k < 3; ++k) P.mR[k] = P.R[k];
+            int lo[3], hi[3];
+            solid_box(a, P.R, P.radius, D, lo, hi);
+            // Keep the stored intervals when no node of the (unchanged) solid box
+            // can change sides: |d^2(R) - d^2(vR)| <= 2 dmax |R - vR| + |R - vR|^2
+            // for every node, dmax its largest distance from vR, and the stored
+            // slack exceeds that bound by far more than the FP64 rounding of d^2.
+            if (a.mode == 0 && P.valid && P.slack > 0.0) {
+                bool same = true;
+                double dlt2 = 0.0, dmax2 = 0.0;
+                for (int k = 0; k < D; ++k) {
+                    same = same && lo[k] == P.slo[k] && hi[k] == P.shi[k];
+                    const double dk = P.R[k] - P.vR[k];
+                    dlt2 += dk * dk;
+                    if (lo[k] <= hi[k]) {
+                        const double e0 = fabs(a.coord[k][lo[k]] - P.vR[k]), e1 = fabs(a.coord[k][hi[k]] - P.vR[k]);
+                        const double e = e0 > e1 ? e0 : e1;
+                        dmax2 += e * e;
+                    }
+                }
+                const double dlt = sqrt(dlt2), dmax = sqrt(dmax2);
+                const double bound = 2.0 * dmax * dlt + dlt2;
+                if (same && bound < P.slack - 1e-9 * (P.r2 + dmax2)) s_keep = 1;
+            }
+        }
+        if (moved && !s_keep) {
+            for (int k = 0; k < 3; ++k) P.vR[k] = P.R[k];
+            P.slack = 0.0;
             int lo[3], hi[3];
             solid_box(a, P.R, P.radius, D, lo, hi);
             bool empty = false;
@@ -269,11 +312,12 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
         P.valid = 1;
     }
     __syncthreads();
-    if (!s_moved) {
+    if (!s_moved || s_keep) {
         // nothing geometric changed; write the record back
         const unsigned long long* ssrc = reinterpret_cast<const unsigned long long*>(&sP);
         unsigned long long* gdst = reinterpret_cast<unsigned long long*>(a.parts + p);
         for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += blockDim.x) gdst[k] = ssrc[k];
+        if (tid == 0) publish_box(a, p, P);
         return;
     }
 
@@ -287,12 +331,17 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
             const int z = P.slo[2] + r / ly;
             const double Y = a.coord[1][y], Z = D == 3 ? a.coord[2][z] : 0.0;
             int xlo = 1, xhi = 0;
+            double slack = 1e300;
             for (int x = lx0; x <= lx1; ++x) {
-                if (sphere_test<D>(a.coord[0][x], Y, Z, P.mR, P.r2)) {
+                const double d2 = sphere_d2<D>(a.coord[0][x], Y, Z, P.vR);
+                if (d2 < P.r2) {
                     if (xlo > xhi) xlo = x;
                     xhi = x;
                 }
+                slack = fmin(slack, fabs(d2 - P.r2));
             }
+            // non-negative doubles order like their bit patterns
+            atomicMin(&s_slack, (unsigned long long)__double_as_longlong(slack));
             int2* slot = a.ivl + P.ivl_off + r;
             const int2 old = *slot;
             if (old.x != xlo || old.y != xhi) changed = 1;
@@ -303,6 +352,7 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
         if (changed) atomicOr(&s_changed, 1);
     }
     __syncthreads();
+    if (tid == 0) P.slack = __longlong_as_double((long long)s_slack);
 
     // 4. boundary-link entries over the near box (solid box + 1, periodic)
     const bool ivl_smem = s_rows <= kIvlSmem;
@@ -366,7 +416,13 @@ __global__ void __launch_bounds__(256) k_particles(const ParticleArgs a) {
         const unsigned long long* ssrc = reinterpret_cast<const unsigned long long*>(&sP);
         unsigned long long* gdst = reinterpret_cast<unsigned long long*>(a.parts + p);
         for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += blockDim.x) gdst[k] = ssrc[k];
+        if (tid == 0) publish_box(a, p, P);
     }
+}
+
+template <class L>
+__global__ void __launch_bounds__(kPartBlock) k_particles(const ParticleArgs a) {
+    particles_body<L>(a, a.mode != 0 ? a.setup_pid : (int)blockIdx.x);
 }
 
 }  // namespace lbm

@@ -23,7 +23,7 @@ struct LbmConfig
     force::NTuple{3,Float64}; force_field::Ptr{Float64}; wall_mask::Ptr{UInt8}
     wall_velocity::Ptr{Float64}; rho_init::Ptr{Float64}; u_init::Ptr{Float64}
     rho_uniform::Float64; u_uniform::NTuple{3,Float64}; rho_ref::Float64; store_scale::Float64
-    device::Int32; reserved0::Int32
+    device::Int32; schedule::Int32
 end
 
 struct LbmParticleParams

@@ -26,6 +26,8 @@ LBM_BEAD, LBM_SQUIRMER = 0, 1
 LBM_FORCE_NONE, LBM_FORCE_UNIFORM, LBM_FORCE_FIELD = 0, 1, 2
 
 STORAGE_NAMES = {"f32": LBM_STORE_F32, "f16": LBM_STORE_F16, "bf16": LBM_STORE_BF16, "f64": LBM_STORE_F64}
+LBM_SCHEDULE_AUTO, LBM_SCHEDULE_STREAM, LBM_SCHEDULE_PERSISTENT = 0, 1, 3
+SCHEDULE_NAMES = {"auto": LBM_SCHEDULE_AUTO, "stream": LBM_SCHEDULE_STREAM, "persistent": LBM_SCHEDULE_PERSISTENT}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -56,7 +58,7 @@ class LbmConfig(C.Structure):
         ("rho_ref", C.c_double),
         ("store_scale", C.c_double),
         ("device", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("schedule", C.c_int32),
     ]
 
 

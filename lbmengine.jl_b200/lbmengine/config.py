@@ -101,7 +101,7 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
                   kineticParameter=0.25, xlims=DEFAULT, ylims=DEFAULT, zlims=DEFAULT, dims=2,
                   walledDimensions=DEFAULT, dampenEcho=False, walls=DEFAULT, movingWalls=DEFAULT,
                   isFluidCompressible=True, forceDensity=DEFAULT, forcingScheme=DEFAULT, saveData=False,
-                  storage="f32", rho_ref=DEFAULT, store_scale=DEFAULT, device=DEFAULT):
+                  storage="f32", rho_ref=DEFAULT, store_scale=DEFAULT, device=DEFAULT, schedule="auto"):
     """Resolve modelInit's keywords (src/gpu/initMethods.jl:440-702) into an LbmConfig.
 
     Returns a namespace with ``cfg`` (capi.LbmConfig), ``keep`` (arrays the
@@ -244,6 +244,9 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
     cfg.rho_ref = 0.0 if rho_ref is DEFAULT else float(rho_ref)
     cfg.store_scale = 0.0 if store_scale is DEFAULT else float(store_scale)
     cfg.device = -1 if device is DEFAULT else int(device)
+    if schedule not in capi.SCHEDULE_NAMES:
+        raise ValueError(f"schedule must be one of {sorted(capi.SCHEDULE_NAMES)}")
+    cfg.schedule = capi.SCHEDULE_NAMES[schedule]
     return SimpleNamespace(cfg=cfg, keep=keep, dt=dt, tau=tau, tau_minus=tau_minus, viscosity=nu,
                            relaxationTimeRatio=ratio, coordinates=axes, shape=shape, dims=dims,
                            velocities=vname, collision=cm, schemes=list(dict.fromkeys(schemes)),

@@ -165,7 +165,9 @@ def modelInit(**kw) -> LBMmodel:
     """modelInit(; ...) — src/gpu/initMethods.jl:440-702.
 
     Extra keywords of this build: ``storage`` ("f32" default, "f16", "bf16",
-    "f64"), ``rho_ref`` and ``store_scale`` (shifted-storage parameters).
+    "f64"), ``rho_ref`` and ``store_scale`` (shifted-storage parameters),
+    ``device`` and ``schedule`` ("auto", "stream", "persistent": how
+    the kernels of a tick are launched; results do not depend on it).
     """
     return LBMmodel(cfgmod.resolve_model(**kw))
 
