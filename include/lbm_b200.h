@@ -253,6 +253,50 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
 int lbm_save_state(lbm_handle* h, const char* path);
 int lbm_load_state(lbm_handle* h, const char* path);
 
+/* ---- batches of independent replicas -------------------------------------
+ * Replicas of one velocity set, collision model and storage format, each with
+ * its own grid, parameters and particles, advanced together: every tick runs
+ * all replicas' bulk tiles, boundary fix-up blocks and particle updates as the
+ * items of one work queue (tick.cuh), either as one persistent launch per
+ * tick or as three queue launches in stream order.  The step loop is replayed
+ * from CUDA graphs.  No counterpart in the reference, which steps one model
+ * per call (parameter sweeps there are loops over modelInit/LBMpropagate!).
+ * Every replica must take the vector bulk path: n[0] a multiple of 4, x-rows
+ * of at most 256 nodes, no per-node force field, not FP64 storage. */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct lbm_batch_tuning {
+    int32_t schedule;     /* LBM_SCHEDULE_STREAM or LBM_SCHEDULE_PERSISTENT */
+    int32_t ctas_per_sm;  /* resident CTAs per SM of the queue kernel (1..occupancy limit) */
+    int32_t tile_order;   /* bulk tiles in the queue: 0 replica by replica, 1 interleaved across replicas */
+    int32_t tile_cta;     /* STREAM only: 1 runs the bulk tiles one CTA each instead of through the queue */
+    double ms_per_tick;   /* device time of one tick measured by lbm_batch_autotune (0 if not measured) */
+} lbm_batch_tuning;
+
+/* n replicas: cfgs[i] with nparticles[i] particles, taken in order from
+ * `particles` (all replicas' particles back to back).  All on one device. */
+int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticles,
+                     const lbm_particle_params* particles, lbm_batch** out);
+int32_t lbm_batch_size(const lbm_batch* b);
+/* Replica i as a model handle, owned by the batch: every lbm_get_* call
+ * works on it, and so does stepping it alone. */
+lbm_handle* lbm_batch_replica(lbm_batch* b, int32_t i);
+/* Advance every replica by nsteps ticks. */
+int lbm_batch_step(lbm_batch* b, int64_t nsteps);
+/* Time every candidate tuning (schedule x bulk kernel x CTAs per SM x tile order) over
+ * `ticks` ticks each, with the state saved before and restored after, and
+ * keep the fastest.  The measured candidates go to results[0..capacity),
+ * their number to *count; the chosen one to *chosen (either may be null). */
+int lbm_batch_autotune(lbm_batch* b, int32_t ticks, lbm_batch_tuning* results, int32_t capacity, int32_t* count,
+                       lbm_batch_tuning* chosen);
+int lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t);
+int lbm_batch_get_tuning(const lbm_batch* b, lbm_batch_tuning* t);
+/* level 0 off, 1 device time of each lbm_batch_step call (lbm_profile.total_ms) */
+int lbm_batch_set_profiling(lbm_batch* b, int32_t level);
+int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out);
+const char* lbm_batch_last_error(const lbm_batch* b);
+void lbm_batch_destroy(lbm_batch* b);
+
 /* Allocation-free stepping.  No counterpart in the reference.
  *
  * Same ticks and results as lbm_step, for callers that must not allocate

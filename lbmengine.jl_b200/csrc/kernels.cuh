@@ -496,10 +496,15 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
     }
 }
 
-// the vector bulk pass over all tiles, one CTA of B threads per tile.
-// Registers are capped at 128 per thread (512 / B resident CTAs).
+// Resident threads per SM the vector bulk kernels are compiled for: a D2Q9
+// thread holds 36 populations and fits 64 registers (32 warps per SM); the
+// 3D sets take up to 128 (16 warps per SM).
+template <class L>
+constexpr int bulk_threads_per_sm() { return L::Q <= 9 ? 1024 : 512; }
+
+// the vector bulk pass over all tiles, one CTA of B threads per tile
 template <class L, int ST, bool TRT, int B>
-__global__ void __launch_bounds__(B, 512 / B) k_bulk_v4(const StepArgs a) {
+__global__ void __launch_bounds__(B, bulk_threads_per_sm<L>() / B) k_bulk_v4(const StepArgs a) {
     __shared__ float s_ex[x_moving_dirs<L>()][B];
     bulk_v4_tile<L, ST, TRT, B>(a, blockIdx.x, s_ex);
 }

@@ -411,6 +411,7 @@ int prepare_tick(lbm_handle* h) {
     h->items.nb = (long long)bm.size();
     h->items.nc = (long long)cm.size();
     h->items.nd = (long long)dm.size();
+    h->items.d_test = 1;
     h->tick_ready = true;
     return LBM_OK;
 }
@@ -1598,5 +1599,562 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
 }
 
 void lbm_destroy(lbm_handle* h) { destroy_all(h); }
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches of independent replicas (lbm_batch_*): the replicas' tick items in
+// one work queue (tick.cuh).
+// ===========================================================================
+struct lbm_batch {
+    int device = 0;
+    std::vector<lbm_handle*> reps;
+    Ops ops{};
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fix = nullptr, ev_part = nullptr;
+    bool part_pending = false;
+    int sms = 0, max_per_sm = 0;
+    lbm_batch_tuning tuning{};
+    // queue items and per-parity arguments, valid while `ready`
+    bool ready = false;
+    std::vector<int> base;  // each replica's buffer index when the items were built
+    int par = 0;            // ticks since then, mod 2
+    int4* d_amap = nullptr;
+    int2 *d_bmap = nullptr, *d_cmap = nullptr, *d_dmap = nullptr;
+    long long na = 0, nb = 0, nc = 0, nd = 0;
+    StepArgs* d_targs = nullptr;      // [2][n]
+    ParticleArgs* d_pargs = nullptr;  // [2][n]
+    TickCounters* d_tq = nullptr;     // [0] main-stream launches, [1] side-stream launches
+    int* d_err = nullptr;             // [n] per replica, plus one for the queue waits
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    int profiling = 0;
+    cudaEvent_t t_begin = nullptr, t_end = nullptr;
+    lbm_profile prof{};
+    long long cells = 0;
+    std::string err;
+};
+
+namespace {
+
+int bset_err(lbm_batch* b, int code, const std::string& msg) {
+    if (b) b->err = msg;
+    else g_global_err = msg;
+    return code;
+}
+
+#define BCUDA_TRY(b, call)                                                                             \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return bset_err((b), e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,         \
+                            std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+        }                                                                                              \
+    } while (0)
+
+template <class P>
+int bdev_alloc(lbm_batch* b, P** p, size_t bytes) {
+    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return bset_err(b, LBM_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    return LBM_OK;
+}
+
+void batch_drop_graphs(lbm_batch* b) {
+    for (auto& g : b->graphs) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+void batch_free_items(lbm_batch* b) {
+    dev_free(b->d_amap);
+    dev_free(b->d_bmap);
+    dev_free(b->d_cmap);
+    dev_free(b->d_dmap);
+    b->ready = false;
+}
+
+// Queue items and arguments of every replica.  Bulk tiles go replica by
+// replica, or interleaved (tile k of every replica, then tile k+1, ...).
+int batch_prepare(lbm_batch* b) {
+    const int n = (int)b->reps.size();
+    bool same = b->ready && (int)b->base.size() == n;
+    for (int r = 0; same && r < n; ++r) same = (b->reps[r]->cur ^ b->base[r]) == b->par;
+    if (same) return LBM_OK;
+    batch_drop_graphs(b);
+    batch_free_items(b);
+    std::vector<int4> am;
+    std::vector<int2> bm, cm, dm;
+    long long maxt = 0;
+    for (int r = 0; r < n; ++r) {
+        lbm_handle* h = b->reps[r];
+        for (long long t = 0; t < (long long)h->vnear.size(); ++t)
+            if (h->vnear[t]) am.push_back(make_int4(r, 0, (int)t, 0));
+        const int np = (int)h->hparts.size();
+        for (int p = 0; p < np; ++p) {
+            const long long len = (long long)std::floor(2.0 * h->hparts[p].radius / h->dx) + 9;
+            const long long nys = std::min<long long>(h->vnt1 + 1, (len + h->vrows - 1) / h->vrows + 2);
+            const long long nzs = h->dims == 3 ? std::min<long long>(h->n[2], len) : 1;
+            if (nys >= 65536 || nzs >= 32768)
+                return bset_err(b, LBM_ERR_UNSUPPORTED, "particle too large for the tick kernel's tile slots");
+            for (long long dz = 0; dz < nzs; ++dz)
+                for (long long dy = 0; dy < nys; ++dy) am.push_back(make_int4(r, 1, p, (int)(dy | (dz << 16))));
+        }
+        const long long nfb = fixup_blocks(h);
+        for (long long k = 0; k < nfb; ++k) bm.push_back(make_int2(r, (int)k));
+        for (int p = 0; p < np; ++p) cm.push_back(make_int2(r, p));
+        maxt = std::max(maxt, h->vtiles);
+    }
+    if (b->tuning.tile_order == 1) {
+        for (long long t = 0; t < maxt; ++t)
+            for (int r = 0; r < n; ++r)
+                if (t < b->reps[r]->vtiles) dm.push_back(make_int2(r, (int)t));
+    } else {
+        for (int r = 0; r < n; ++r)
+            for (long long t = 0; t < b->reps[r]->vtiles; ++t) dm.push_back(make_int2(r, (int)t));
+    }
+    std::vector<StepArgs> ta(2 * (size_t)n);
+    std::vector<ParticleArgs> pa(2 * (size_t)n);
+    b->base.resize(n);
+    for (int r = 0; r < n; ++r) {
+        lbm_handle* h = b->reps[r];
+        b->base[r] = h->cur;
+        for (int s = 0; s < 2; ++s) {
+            const int src = h->cur ^ s;
+            StepArgs& a = ta[(size_t)s * n + r];
+            a = step_args(h, src);
+            a.nbox = h->d_nbox[1 - src];
+            a.err = b->d_err + r;
+            ParticleArgs& q = pa[(size_t)s * n + r];
+            q = particle_args(h, 0, 0, src);
+            q.err = b->d_err + r;
+        }
+    }
+    b->par = 0;
+    int rc = bdev_alloc(b, &b->d_amap, sizeof(int4) * std::max<size_t>(1, am.size()));
+    if (!rc) rc = bdev_alloc(b, &b->d_bmap, sizeof(int2) * std::max<size_t>(1, bm.size()));
+    if (!rc) rc = bdev_alloc(b, &b->d_cmap, sizeof(int2) * std::max<size_t>(1, cm.size()));
+    if (!rc) rc = bdev_alloc(b, &b->d_dmap, sizeof(int2) * std::max<size_t>(1, dm.size()));
+    if (rc) return rc;
+    if (!am.empty()) BCUDA_TRY(b, cudaMemcpyAsync(b->d_amap, am.data(), sizeof(int4) * am.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!bm.empty()) BCUDA_TRY(b, cudaMemcpyAsync(b->d_bmap, bm.data(), sizeof(int2) * bm.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!cm.empty()) BCUDA_TRY(b, cudaMemcpyAsync(b->d_cmap, cm.data(), sizeof(int2) * cm.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!dm.empty()) BCUDA_TRY(b, cudaMemcpyAsync(b->d_dmap, dm.data(), sizeof(int2) * dm.size(), cudaMemcpyHostToDevice, b->stream));
+    BCUDA_TRY(b, cudaMemcpyAsync(b->d_targs, ta.data(), sizeof(StepArgs) * ta.size(), cudaMemcpyHostToDevice, b->stream));
+    BCUDA_TRY(b, cudaMemcpyAsync(b->d_pargs, pa.data(), sizeof(ParticleArgs) * pa.size(), cudaMemcpyHostToDevice, b->stream));
+    BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    b->na = (long long)am.size();
+    b->nb = (long long)bm.size();
+    b->nc = (long long)cm.size();
+    b->nd = (long long)dm.size();
+    b->ready = true;
+    return LBM_OK;
+}
+
+TickItems batch_items(const lbm_batch* b, bool a, bool bb, bool c, bool d, int d_test) {
+    TickItems it{};
+    it.amap = b->d_amap;
+    it.bmap = b->d_bmap;
+    it.cmap = b->d_cmap;
+    it.dmap = b->d_dmap;
+    it.na = a ? b->na : 0;
+    it.nb = bb ? b->nb : 0;
+    it.nc = c ? b->nc : 0;
+    it.nd = d ? b->nd : 0;
+    it.d_test = d_test;
+    // items past the enabled phases are addressed from the start of their map
+    if (!a) it.amap = nullptr;
+    return it;
+}
+
+void batch_launch(lbm_batch* b, int s, const TickItems& it, int q, cudaStream_t st) {
+    const long long items = it.na + it.nb + it.nc + it.nd;
+    if (items == 0) return;
+    const long long cap = (long long)std::max(1, b->tuning.ctas_per_sm) * b->sms;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min(items, cap));
+    const size_t n = b->reps.size();
+    b->ops.tick(b->d_targs + (size_t)s * n, b->d_pargs + (size_t)s * n, it, b->d_tq + q,
+                b->d_err + n, grid, st);
+}
+
+// one tick of every replica with arguments of parity s (capturable)
+void batch_enqueue(lbm_batch* b, int s) {
+    if (b->tuning.schedule == LBM_SCHEDULE_PERSISTENT) {
+        batch_launch(b, s, batch_items(b, true, true, true, true, 1), 0, b->stream);
+        return;
+    }
+    // stream order: all tiles; then the fix-up blocks once the previous
+    // particle update is done; the particle update on the side stream
+    if (b->tuning.tile_cta)
+        b->ops.bulk_batch(b->d_targs + (size_t)s * b->reps.size(), b->d_dmap, b->nd, b->stream);
+    else
+        batch_launch(b, s, batch_items(b, false, false, false, true, 0), 0, b->stream);
+    if (b->part_pending) {
+        cudaStreamWaitEvent(b->stream, b->ev_part, 0);
+        b->part_pending = false;
+    }
+    if (b->nb > 0) batch_launch(b, s, batch_items(b, false, true, false, false, 0), 0, b->stream);
+    if (b->nc > 0) {
+        cudaEventRecord(b->ev_fix, b->stream);
+        cudaStreamWaitEvent(b->side, b->ev_fix, 0);
+        batch_launch(b, s, batch_items(b, false, false, true, false, 0), 1, b->side);
+        cudaEventRecord(b->ev_part, b->side);
+        b->part_pending = true;
+    }
+}
+
+void batch_join(lbm_batch* b) {
+    if (b->part_pending) {
+        cudaStreamWaitEvent(b->stream, b->ev_part, 0);
+        b->part_pending = false;
+    }
+}
+
+int batch_graph(lbm_batch* b, int s0) {
+    if (b->graphs[s0]) return LBM_OK;
+    cudaGraph_t graph = nullptr;
+    BCUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kGraphSteps; ++k) batch_enqueue(b, s0 ^ (k & 1));
+    batch_join(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bset_err(b, LBM_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+    }
+    e = cudaGraphInstantiate(&b->graphs[s0], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        b->graphs[s0] = nullptr;
+        return bset_err(b, LBM_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+    }
+    return LBM_OK;
+}
+
+int batch_check(lbm_batch* b) {
+    const size_t n = b->reps.size();
+    std::vector<int> err(n + 1, 0);
+    BCUDA_TRY(b, cudaMemcpyAsync(err.data(), b->d_err, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, b->stream));
+    BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    if (err[n] & kErrSpinTimeout) return bset_err(b, LBM_ERR_TIMEOUT, "a wait inside the tick kernel gave up");
+    for (size_t r = 0; r < n; ++r) {
+        if (err[r] & kErrLinkOverflow)
+            return bset_err(b, LBM_ERR_STATE, "replica " + std::to_string(r) + ": particle links exceeded their capacity");
+        if (err[r] & kErrIntervalOverflow)
+            return bset_err(b, LBM_ERR_STATE, "replica " + std::to_string(r) + ": particle solid box exceeded its capacity");
+    }
+    return LBM_OK;
+}
+
+// run `ticks` ticks without touching the replicas' tick counters; the caller
+// restores the state
+int batch_run_raw(lbm_batch* b, int ticks, float* ms) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BCUDA_TRY(b, cudaEventCreate(&e0));
+    BCUDA_TRY(b, cudaEventCreate(&e1));
+    int s = b->par;
+    for (int k = 0; k < 3; ++k, s ^= 1) batch_enqueue(b, s);  // warm-up
+    batch_join(b);
+    BCUDA_TRY(b, cudaEventRecord(e0, b->stream));
+    for (int k = 0; k < ticks; ++k, s ^= 1) batch_enqueue(b, s);
+    batch_join(b);
+    BCUDA_TRY(b, cudaEventRecord(e1, b->stream));
+    BCUDA_TRY(b, cudaEventSynchronize(e1));
+    BCUDA_TRY(b, cudaGetLastError());
+    BCUDA_TRY(b, cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return LBM_OK;
+}
+
+// everything a tick writes, for every replica: into / out of one device buffer
+int batch_snapshot(lbm_batch* b, char** buf, size_t* bytes, bool save) {
+    auto regions = [](lbm_handle* h, std::vector<std::pair<void*, size_t>>& v) {
+        const size_t pop = (size_t)h->N * h->q * storage_bytes(h->storage);
+        const size_t np = h->hparts.size();
+        v.push_back({h->pop[0], pop});
+        v.push_back({h->pop[1], pop});
+        v.push_back({h->d_parts, sizeof(ParticleDev) * np});
+        v.push_back({h->d_ivl, sizeof(int2) * h->ivl_slots});
+        v.push_back({h->d_links, sizeof(int2) * h->link_slots});
+        v.push_back({h->d_tilebits, sizeof(unsigned long long) * h->g.ntiles * h->words});
+        v.push_back({h->d_nbox[0], sizeof(int) * 6 * np});
+        v.push_back({h->d_nbox[1], sizeof(int) * 6 * np});
+    };
+    std::vector<std::pair<void*, size_t>> v;
+    for (lbm_handle* h : b->reps) regions(h, v);
+    if (save) {
+        size_t total = 0;
+        for (auto& r : v) total += (r.first ? r.second : 0);
+        int rc = bdev_alloc(b, buf, total);
+        if (rc) return rc;
+        *bytes = total;
+    }
+    char* p = *buf;
+    for (auto& r : v) {
+        if (!r.first || !r.second) continue;
+        if (save) BCUDA_TRY(b, cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToDevice, b->stream));
+        else BCUDA_TRY(b, cudaMemcpyAsync(r.first, p, r.second, cudaMemcpyDeviceToDevice, b->stream));
+        p += r.second;
+    }
+    BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    return LBM_OK;
+}
+
+void batch_destroy_all(lbm_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->side) cudaStreamSynchronize(b->side);
+    batch_drop_graphs(b);
+    batch_free_items(b);
+    dev_free(b->d_targs);
+    dev_free(b->d_pargs);
+    dev_free(b->d_tq);
+    dev_free(b->d_err);
+    if (b->t_begin) cudaEventDestroy(b->t_begin);
+    if (b->t_end) cudaEventDestroy(b->t_end);
+    if (b->ev_fix) cudaEventDestroy(b->ev_fix);
+    if (b->ev_part) cudaEventDestroy(b->ev_part);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (lbm_handle* h : b->reps) destroy_all(h);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticles,
+                     const lbm_particle_params* particles, lbm_batch** out) {
+    if (!out || !cfgs || n < 1) return bset_err(nullptr, LBM_ERR_INVALID, "a batch needs at least one replica");
+    *out = nullptr;
+    lbm_batch* b = new lbm_batch();
+    b->tuning.schedule = LBM_SCHEDULE_PERSISTENT;
+    b->tuning.tile_order = 0;
+    long long k = 0;
+    for (int r = 0; r < n; ++r) {
+        lbm_config c = cfgs[r];
+        c.schedule = LBM_SCHEDULE_STREAM;
+        lbm_handle* h = nullptr;
+        int rc = lbm_create(&c, &h);
+        if (rc) {
+            const std::string m = "replica " + std::to_string(r) + ": " + g_global_err;
+            batch_destroy_all(b);
+            return bset_err(nullptr, rc, m);
+        }
+        b->reps.push_back(h);
+        const int np = nparticles ? nparticles[r] : 0;
+        for (int p = 0; p < np; ++p, ++k) {
+            rc = lbm_add_particle(h, particles + k, nullptr);
+            if (rc) {
+                const std::string m = "replica " + std::to_string(r) + ", particle " + std::to_string(p) + ": " + h->err;
+                batch_destroy_all(b);
+                return bset_err(nullptr, rc, m);
+            }
+        }
+        const lbm_handle* h0 = b->reps[0];
+        std::string why;
+        if (!use_vector_bulk(h) || h->vblock != kTickBlock || !h->ops.tick) why = "needs the vector bulk path with x-rows of at most 256 nodes";
+        else if (h->device != h0->device) why = "all replicas must be on one device";
+        else if (h->lattice != h0->lattice || h->storage != h0->storage || h->trt != h0->trt)
+            why = "all replicas must share the velocity set, storage format and collision model";
+        if (!why.empty()) {
+            batch_destroy_all(b);
+            return bset_err(nullptr, LBM_ERR_UNSUPPORTED, "replica " + std::to_string(r) + ": " + why);
+        }
+        b->cells += h->N;
+    }
+    b->device = b->reps[0]->device;
+    b->ops = b->reps[0]->ops;
+    cudaSetDevice(b->device);
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    int rc = LBM_OK;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fix, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_part, cudaEventDisableTiming) != cudaSuccess)
+        rc = bset_err(b, LBM_ERR_CUDA, "stream or event creation failed");
+    if (!rc) rc = bdev_alloc(b, &b->d_targs, sizeof(StepArgs) * 2 * n);
+    if (!rc) rc = bdev_alloc(b, &b->d_pargs, sizeof(ParticleArgs) * 2 * n);
+    if (!rc) rc = bdev_alloc(b, &b->d_tq, sizeof(TickCounters) * 2);
+    if (!rc) rc = bdev_alloc(b, &b->d_err, sizeof(int) * (n + 1));
+    if (!rc && (cudaMemset(b->d_tq, 0, sizeof(TickCounters) * 2) != cudaSuccess ||
+                cudaMemset(b->d_err, 0, sizeof(int) * (n + 1)) != cudaSuccess))
+        rc = bset_err(b, LBM_ERR_CUDA, "memset failed");
+    if (!rc && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->max_per_sm, b->ops.tick_fn, kTickBlock, 0) != cudaSuccess ||
+                cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess))
+        rc = bset_err(b, LBM_ERR_CUDA, "occupancy query failed");
+    if (rc) {
+        const std::string m = b->err;
+        batch_destroy_all(b);
+        return bset_err(nullptr, rc, m);
+    }
+    b->tuning.ctas_per_sm = std::max(1, b->max_per_sm);
+    *out = b;
+    return LBM_OK;
+}
+
+int32_t lbm_batch_size(const lbm_batch* b) { return b ? (int32_t)b->reps.size() : 0; }
+
+lbm_handle* lbm_batch_replica(lbm_batch* b, int32_t i) {
+    if (!b || i < 0 || i >= (int32_t)b->reps.size()) return nullptr;
+    return b->reps[i];
+}
+
+int lbm_batch_step(lbm_batch* b, int64_t nsteps) {
+    if (!b) return bset_err(b, LBM_ERR_INVALID, "null batch");
+    if (nsteps < 0) return bset_err(b, LBM_ERR_INVALID, "ticks must be non-negative");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, LBM_ERR_CUDA, "cannot select the batch's device");
+    for (lbm_handle* h : b->reps) {  // work a replica stepped alone left on its streams
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bset_err(b, LBM_ERR_CUDA, "replica stream failed");
+    }
+    int rc = batch_prepare(b);
+    if (rc) return rc;
+    if (b->profiling) BCUDA_TRY(b, cudaEventRecord(b->t_begin, b->stream));
+    int64_t done = 0;
+    while (nsteps - done >= kGraphSteps) {
+        rc = batch_graph(b, b->par);
+        if (rc) return rc;
+        BCUDA_TRY(b, cudaGraphLaunch(b->graphs[b->par], b->stream));
+        done += kGraphSteps;  // even: the parity is unchanged
+    }
+    for (; done < nsteps; ++done) {
+        batch_enqueue(b, b->par);
+        b->par ^= 1;
+    }
+    batch_join(b);
+    if (b->profiling) BCUDA_TRY(b, cudaEventRecord(b->t_end, b->stream));
+    BCUDA_TRY(b, cudaGetLastError());
+    for (lbm_handle* h : b->reps) {
+        if (nsteps & 1) h->cur ^= 1;
+        h->tick += nsteps;
+        for (int64_t s = 0; s < nsteps; ++s) h->time += h->dt;
+    }
+    rc = batch_check(b);
+    b->prof = lbm_profile{};
+    b->prof.steps = nsteps;
+    b->prof.bulk_cells = b->cells;
+    b->prof.launches = nsteps * (b->tuning.schedule == LBM_SCHEDULE_PERSISTENT
+                                     ? 1 : 1 + (b->nb > 0 ? 1 : 0) + (b->nc > 0 ? 1 : 0));
+    if (b->profiling && nsteps > 0) {
+        float ms = 0;
+        BCUDA_TRY(b, cudaEventElapsedTime(&ms, b->t_begin, b->t_end));
+        b->prof.total_ms = ms;
+    }
+    return rc;
+}
+
+int lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t) {
+    if (!b || !t) return bset_err(b, LBM_ERR_INVALID, "null argument");
+    if ((t->schedule != LBM_SCHEDULE_STREAM && t->schedule != LBM_SCHEDULE_PERSISTENT) || t->ctas_per_sm < 1 ||
+        t->ctas_per_sm > std::max(1, b->max_per_sm) || t->tile_order < 0 || t->tile_order > 1 || t->tile_cta < 0 ||
+        t->tile_cta > 1)
+        return bset_err(b, LBM_ERR_INVALID, "invalid tuning");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, LBM_ERR_CUDA, "cannot select the batch's device");
+    BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    const bool reorder = t->tile_order != b->tuning.tile_order;
+    b->tuning = *t;
+    batch_drop_graphs(b);
+    if (reorder) batch_free_items(b);
+    return LBM_OK;
+}
+
+int lbm_batch_get_tuning(const lbm_batch* b, lbm_batch_tuning* t) {
+    if (!b || !t) return LBM_ERR_INVALID;
+    *t = b->tuning;
+    return LBM_OK;
+}
+
+int lbm_batch_autotune(lbm_batch* b, int32_t ticks, lbm_batch_tuning* results, int32_t capacity, int32_t* count,
+                       lbm_batch_tuning* chosen) {
+    if (!b || ticks < 1) return bset_err(b, LBM_ERR_INVALID, "autotune needs a batch and at least one tick");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, LBM_ERR_CUDA, "cannot select the batch's device");
+    for (lbm_handle* h : b->reps) BCUDA_TRY(b, cudaStreamSynchronize(h->stream));
+    int rc = batch_prepare(b);
+    if (rc) return rc;
+    char* save = nullptr;
+    size_t bytes = 0;
+    rc = batch_snapshot(b, &save, &bytes, true);
+    if (rc) return rc;
+    std::vector<lbm_batch_tuning> cand;
+    std::vector<int> per_sm;
+    for (int c : {2, 4, 6, 8, 12, 16})
+        if (c <= b->max_per_sm) per_sm.push_back(c);
+    if (per_sm.empty() || per_sm.back() != b->max_per_sm) per_sm.push_back(b->max_per_sm);
+    for (int sched : {LBM_SCHEDULE_PERSISTENT, LBM_SCHEDULE_STREAM})
+        for (int cta : {0, 1}) {
+            if (sched == LBM_SCHEDULE_PERSISTENT && cta) continue;  // everything goes through the queue
+            for (int order : {0, 1})
+                for (int c : per_sm) {
+                    lbm_batch_tuning t{};
+                    t.schedule = sched;
+                    t.ctas_per_sm = c;
+                    t.tile_order = order;
+                    t.tile_cta = cta;
+                    cand.push_back(t);
+                }
+        }
+    const lbm_batch_tuning keep = b->tuning;
+    int best = -1;
+    for (size_t i = 0; i < cand.size(); ++i) {
+        if (cand[i].tile_order != b->tuning.tile_order) {
+            b->tuning.tile_order = cand[i].tile_order;
+            batch_free_items(b);
+            rc = batch_prepare(b);
+            if (rc) break;
+        }
+        b->tuning = cand[i];
+        float ms = 0;
+        rc = batch_run_raw(b, ticks, &ms);
+        if (!rc) rc = batch_snapshot(b, &save, &bytes, false);  // restore
+        if (!rc) rc = batch_check(b);
+        if (rc) break;
+        cand[i].ms_per_tick = ms / ticks;
+        if (best < 0 || cand[i].ms_per_tick < cand[best].ms_per_tick) best = (int)i;
+    }
+    dev_free(save);
+    batch_drop_graphs(b);
+    if (rc || best < 0) {
+        b->tuning = keep;
+        batch_free_items(b);
+        return rc ? rc : bset_err(b, LBM_ERR_STATE, "no tuning candidate ran");
+    }
+    if (cand[best].tile_order != b->tuning.tile_order) batch_free_items(b);
+    b->tuning = cand[best];
+    if (results && count) {
+        const int m = std::min<int>(capacity, (int)cand.size());
+        for (int i = 0; i < m; ++i) results[i] = cand[i];
+    }
+    if (count) *count = (int32_t)cand.size();
+    if (chosen) *chosen = cand[best];
+    return LBM_OK;
+}
+
+int lbm_batch_set_profiling(lbm_batch* b, int32_t level) {
+    if (!b) return LBM_ERR_INVALID;
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, LBM_ERR_CUDA, "cannot select the batch's device");
+    if (level > 0 && !b->t_begin) {
+        BCUDA_TRY(b, cudaEventCreate(&b->t_begin));
+        BCUDA_TRY(b, cudaEventCreate(&b->t_end));
+    }
+    b->profiling = level > 0 ? 1 : 0;
+    return LBM_OK;
+}
+
+int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out) {
+    if (!b || !out) return LBM_ERR_INVALID;
+    *out = b->prof;
+    return LBM_OK;
+}
+
+const char* lbm_batch_last_error(const lbm_batch* b) { return b ? b->err.c_str() : g_global_err.c_str(); }
+
+void lbm_batch_destroy(lbm_batch* b) { batch_destroy_all(b); }
 
 }  // extern "C"

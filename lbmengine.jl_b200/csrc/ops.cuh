@@ -24,6 +24,8 @@ struct Ops {
     // one persistent kernel per tick over the A/B/C/D item queue (tick.cuh)
     void (*tick)(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
                  int* err, unsigned grid, cudaStream_t);
+    // a batch's bulk tiles, one CTA per entry of dmap
+    void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
     const void* fixup_fn;
     const void* tick_fn;
@@ -57,6 +59,9 @@ struct OpsImpl {
                      int* err, unsigned grid, cudaStream_t s) {
         if constexpr (ST != ST_F64) k_tick<L, ST, TRT><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
     }
+    static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s) {
+        if constexpr (ST != ST_F64) k_bulk_batch<L, ST, TRT><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+    }
     static void encode(const CodecArgs& a, cudaStream_t s) { k_encode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void macro(const CodecArgs& a, cudaStream_t s) { k_macro<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
@@ -78,6 +83,7 @@ struct OpsImpl {
         o.mask = mask;
         o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
         o.tick = ST == ST_F64 ? nullptr : tick;
+        o.bulk_batch = ST == ST_F64 ? nullptr : bulk_batch;
         o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
         o.fixup_fn = (const void*)k_fixup<L, ST, TRT>;
         o.tick_fn = nullptr;

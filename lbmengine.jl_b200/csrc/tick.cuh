@@ -19,6 +19,8 @@
 // and finish without waiting on later ones, so the waits always end; each
 // wait is bounded anyway and reports kErrSpinTimeout if it gives up.
 // Replicas of a batch simply contribute their items to the same four phases.
+// The same kernel also runs subsets of the queue (only D items over every
+// tile, only B items, only C items) as three launches in stream order.
 //
 // The particle update of tick n runs while the D tiles of tick n still test
 // particle boxes, so it publishes its boxes into the other of two buffers:
@@ -39,6 +41,8 @@ struct TickItems {
     const int2* cmap;  // {replica, particle}
     const int2* dmap;  // {replica, tile}
     long long na, nb, nc, nd;
+    int d_test;  // 1: D items skip tiles near boundary work (A covers them); 0: D is every tile
+    int pad;
 };
 
 struct TickCounters {
@@ -153,9 +157,13 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
         } else {
             const int2 m = it.dmap[t - nabc];
             const StepArgs& A = args[m.x];
-            bool nr = threadIdx.x == 0 && A.vnear && A.vnear[m.y];
-            for (int p = threadIdx.x; p < A.nparts; p += B) nr = nr || tile_meets_box<L::D>(A, m.y, p);
-            if (!__syncthreads_or(nr)) bulk_v4_tile<L, ST, TRT, B>(A, m.y, s_ex);
+            bool skip = false;
+            if (it.d_test) {
+                bool nr = threadIdx.x == 0 && A.vnear && A.vnear[m.y];
+                for (int p = threadIdx.x; p < A.nparts; p += B) nr = nr || tile_meets_box<L::D>(A, m.y, p);
+                skip = __syncthreads_or(nr);
+            }
+            if (!skip) bulk_v4_tile<L, ST, TRT, B>(A, m.y, s_ex);
         }
         if (threadIdx.x == 0) s_next = nxt;
         __syncthreads();
@@ -171,6 +179,16 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
             __threadfence();
         }
     }
+}
+
+// The bulk tiles of a batch, one CTA per item of the D map (no queue): the
+// replicas' arguments come from `args[dmap[i].x]`.
+template <class L, int ST, bool TRT>
+__global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L>() / kTickBlock)
+    k_bulk_batch(const StepArgs* __restrict__ args, const int2* __restrict__ dmap) {
+    __shared__ float s_ex[x_moving_dirs<L>()][kTickBlock];
+    const int2 m = dmap[blockIdx.x];
+    bulk_v4_tile<L, ST, TRT, kTickBlock>(args[m.x], m.y, s_ex);
 }
 
 }  // namespace lbm

@@ -11,7 +11,8 @@ The compute path is liblbm_b200.so (CUDA, sm_100a), loaded through ctypes.
 from .config import DEFAULT, julia_float_range, resolve_bead, resolve_model, resolve_squirmer  # noqa: F401
 from .model import (LBMmodel, LBMparticle, LBMpropagate, addBead, addSquirmer,  # noqa: F401
                     hydroVariablesUpdate, modelInit)
+from .batch import LBMbatch  # noqa: F401
 from . import _capi  # noqa: F401
 
 __all__ = ["modelInit", "addSquirmer", "addBead", "LBMpropagate", "hydroVariablesUpdate", "LBMmodel",
-           "LBMparticle", "DEFAULT"]
+           "LBMparticle", "LBMbatch", "DEFAULT"]

@@ -129,6 +129,16 @@ class LbmProfile(C.Structure):
     ]
 
 
+class LbmBatchTuning(C.Structure):
+    _fields_ = [
+        ("schedule", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("tile_order", C.c_int32),
+        ("tile_cta", C.c_int32),
+        ("ms_per_tick", C.c_double),
+    ]
+
+
 # (name, restype, argtypes) for every symbol of include/lbm_b200.h
 PROTOTYPES = [
     ("lbm_abi_version", C.c_int32, []),
@@ -154,6 +164,19 @@ PROTOTYPES = [
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_last_global_error", C.c_char_p, []),
     ("lbm_destroy", None, [C.c_void_p]),
+    ("lbm_batch_create", C.c_int, [C.c_int32, C.POINTER(LbmConfig), C.POINTER(C.c_int32),
+                                   C.POINTER(LbmParticleParams), C.POINTER(C.c_void_p)]),
+    ("lbm_batch_size", C.c_int32, [C.c_void_p]),
+    ("lbm_batch_replica", C.c_void_p, [C.c_void_p, C.c_int32]),
+    ("lbm_batch_step", C.c_int, [C.c_void_p, C.c_int64]),
+    ("lbm_batch_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(LbmBatchTuning), C.c_int32,
+                                     C.POINTER(C.c_int32), C.POINTER(LbmBatchTuning)]),
+    ("lbm_batch_set_tuning", C.c_int, [C.c_void_p, C.POINTER(LbmBatchTuning)]),
+    ("lbm_batch_get_tuning", C.c_int, [C.c_void_p, C.POINTER(LbmBatchTuning)]),
+    ("lbm_batch_set_profiling", C.c_int, [C.c_void_p, C.c_int32]),
+    ("lbm_batch_get_profile", C.c_int, [C.c_void_p, C.POINTER(LbmProfile)]),
+    ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("lbm_batch_destroy", None, [C.c_void_p]),
 ]
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

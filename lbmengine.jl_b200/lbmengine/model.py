@@ -25,11 +25,17 @@ class LBMparticle(SimpleNamespace):
 class LBMmodel:
     """A model living on the GPU (LBMmodel, src/gpu/structs.jl:52-76)."""
 
-    def __init__(self, resolved, lib=None):
+    def __init__(self, resolved, lib=None, handle=None):
+        """Create the model on the GPU, or (``handle``) wrap a replica handle a
+        batch owns; such a view never destroys it."""
         self._lib = lib or capi.load()
         self._res = resolved
-        self._h = C.c_void_p()
-        capi.check(self._lib, None, self._lib.lbm_create(C.byref(resolved.cfg), C.byref(self._h)))
+        self._owned = handle is None
+        if handle is None:
+            self._h = C.c_void_p()
+            capi.check(self._lib, None, self._lib.lbm_create(C.byref(resolved.cfg), C.byref(self._h)))
+        else:
+            self._h = C.c_void_p(handle)
         self.schemes = list(resolved.schemes)
         self.spaceTime = SimpleNamespace(coordinates=resolved.coordinates, latticeParameter=resolved.dt,
                                          timeStep=resolved.dt, latticeSpeed=1.0, dims=resolved.dims)
@@ -58,9 +64,9 @@ class LBMmodel:
         return self._h
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             self._lib.lbm_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
