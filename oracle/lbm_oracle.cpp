@@ -30,6 +30,17 @@
  * (left to right, no fused multiply-add: build with -ffp-contract=off).
  * Reductions the reference does with CUDA.jl parallel sums are done here
  * sequentially in column-major cell order.
+ *
+ * The model is a template on its scalar type.  With `double` it is the FP64
+ * oracle (orc_* entry points).  With Dual<kDirs> (forward-mode dual numbers,
+ * value + kDirs directional derivatives) it carries the derivatives of the
+ * whole trajectory with respect to seeded parameters (ord_* entry points):
+ * the value parts follow exactly the operations of the FP64 run, every
+ * comparison (masks, zero tests) looks at the value part only, so the
+ * derivatives are those of the reference's tick with its solid masks held as
+ * computed.  The reference's CPU module is hard-typed Float64
+ * (src/cpu/structs.jl:14-37), so dual numbers cannot flow through the Julia
+ * code itself; they flow through this restatement.
  */
 #include "lbm_b200.h"
 #include "lattice_tables.h"
@@ -51,39 +62,103 @@ namespace {
 
 thread_local std::string g_err;
 
+// ---- forward-mode dual numbers ---------------------------------------------
+constexpr int kDirs = 6;  // derivative directions carried by the dual oracle
+
+template <int K>
+struct Dual {
+    double v = 0.0;
+    double d[K] = {};
+    Dual() = default;
+    Dual(double x) : v(x) {}  // NOLINT: constants enter as duals with zero derivatives
+    Dual& operator+=(const Dual& o) { v += o.v; for (int k = 0; k < K; ++k) d[k] += o.d[k]; return *this; }
+    Dual& operator-=(const Dual& o) { v -= o.v; for (int k = 0; k < K; ++k) d[k] -= o.d[k]; return *this; }
+};
+template <int K> Dual<K> operator+(Dual<K> a, const Dual<K>& b) { a += b; return a; }
+template <int K> Dual<K> operator-(Dual<K> a, const Dual<K>& b) { a -= b; return a; }
+template <int K> Dual<K> operator-(const Dual<K>& a) { Dual<K> r; r.v = -a.v; for (int k = 0; k < K; ++k) r.d[k] = -a.d[k]; return r; }
+template <int K> Dual<K> operator*(const Dual<K>& a, const Dual<K>& b) {
+    Dual<K> r; r.v = a.v * b.v;
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+template <int K> Dual<K> operator/(const Dual<K>& a, const Dual<K>& b) {
+    Dual<K> r; r.v = a.v / b.v;
+    for (int k = 0; k < K; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+    return r;
+}
+template <int K> Dual<K> operator+(Dual<K> a, double b) { a.v += b; return a; }
+template <int K> Dual<K> operator+(double b, Dual<K> a) { a.v = b + a.v; return a; }
+template <int K> Dual<K> operator-(Dual<K> a, double b) { a.v -= b; return a; }
+template <int K> Dual<K> operator-(double b, const Dual<K>& a) { return Dual<K>(b) - a; }
+template <int K> Dual<K> operator*(Dual<K> a, double b) { a.v *= b; for (int k = 0; k < K; ++k) a.d[k] *= b; return a; }
+template <int K> Dual<K> operator*(double b, Dual<K> a) { a.v = b * a.v; for (int k = 0; k < K; ++k) a.d[k] = b * a.d[k]; return a; }
+template <int K> Dual<K> operator/(Dual<K> a, double b) { a.v /= b; for (int k = 0; k < K; ++k) a.d[k] /= b; return a; }
+template <int K> Dual<K> operator/(double b, const Dual<K>& a) { return Dual<K>(b) / a; }
+template <int K> bool operator==(const Dual<K>& a, double b) { return a.v == b; }
+template <int K> bool operator!=(const Dual<K>& a, double b) { return a.v != b; }
+template <int K> Dual<K> sqrt(const Dual<K>& a) {
+    Dual<K> r; r.v = std::sqrt(a.v);
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] / (2.0 * r.v);
+    return r;
+}
+template <int K> Dual<K> fabs(const Dual<K>& a) { return a.v < 0 ? -a : a; }
+template <int K> Dual<K> sin(const Dual<K>& a) {
+    Dual<K> r; r.v = std::sin(a.v); const double c = std::cos(a.v);
+    for (int k = 0; k < K; ++k) r.d[k] = c * a.d[k];
+    return r;
+}
+template <int K> Dual<K> cos(const Dual<K>& a) {
+    Dual<K> r; r.v = std::cos(a.v); const double sn = std::sin(a.v);
+    for (int k = 0; k < K; ++k) r.d[k] = -sn * a.d[k];
+    return r;
+}
+inline double val(double x) { return x; }
+template <int K> double val(const Dual<K>& x) { return x.v; }
+using std::cos;
+using std::fabs;
+using std::sin;
+using std::sqrt;
+using D6 = Dual<kDirs>;
+
 int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
 
+template <class Real>
 struct Particle {
     int id = 0;
     int kind = LBM_SQUIRMER;
     bool couple_f = false, couple_t = false;
-    double radius = 0, B1 = 0, B2 = 0;
+    double radius = 0;
+    Real B1 = 0, B2 = 0;
     double inv_mass = 0, inv_inertia = 0;
-    double R[3] = {0, 0, 0}, v[3] = {0, 0, 0}, w[3] = {0, 0, 0}, e[3] = {0, 0, 0};
-    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};  // forceInput / torqueInput
-    double lastF[3] = {0, 0, 0}, lastT[3] = {0, 0, 0};
+    Real R[3] = {0, 0, 0}, v[3] = {0, 0, 0}, w[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+    Real F[3] = {0, 0, 0}, T[3] = {0, 0, 0};  // forceInput / torqueInput
+    Real lastF[3] = {0, 0, 0}, lastT[3] = {0, 0, 0};
     std::vector<uint8_t> S;  // solidRegion
     // state captured by the last getNodeVelocity call (nodeVelocity is a
     // function of it, evaluated on demand)
-    double nvR[3] = {0, 0, 0}, nvV[3] = {0, 0, 0}, nvW[3] = {0, 0, 0}, nvE[3] = {0, 0, 0};
+    Real nvR[3] = {0, 0, 0}, nvV[3] = {0, 0, 0}, nvW[3] = {0, 0, 0}, nvE[3] = {0, 0, 0};
 };
 
+template <class Real>
 struct Model {
     int dims = 0;
     VelocitySet vs;
     int64_t n[3] = {1, 1, 1};
     int64_t N = 0;
     std::vector<double> X[3];
-    double dx = 1, dt = 1, tau = 1, tau_plus = 1, tau_minus = 1;
+    double dx = 1, dt = 1;
+    Real tau = 1, tau_plus = 1, tau_minus = 1;
     double invC2 = 3, invC4 = 9;
     bool trt = false, compressible = true;
     bool bounce_back = false, moving_walls = false, guo = false, ladd = false;
-    std::vector<double> f, rho, u, F, rho0, uw;
+    std::vector<Real> f, rho, u, F, rho0;
+    std::vector<double> uw;
     std::vector<uint8_t> W;
-    std::vector<Particle> parts;
+    std::vector<Particle<Real>> parts;
     int64_t tick = 0;
     double time = 0;
 
@@ -111,13 +186,15 @@ struct Model {
 };
 
 // getSphere: ((X1-R1)^2 + (X2-R2)^2 [+ (X3-R3)^2]) < r^2, kernels.jl:335-353.
-// X + (-R) equals X - R exactly in IEEE arithmetic.
-inline bool in_sphere(const Model& m, int64_t x, int64_t y, int64_t z, const double* R, double r2) {
-    double a = m.X[0][x] - R[0];
-    double b = m.X[1][y] - R[1];
+// X + (-R) equals X - R exactly in IEEE arithmetic.  The test is a comparison:
+// it uses the value part of the position.
+template <class Real>
+inline bool in_sphere(const Model<Real>& m, int64_t x, int64_t y, int64_t z, const Real* R, double r2) {
+    double a = m.X[0][x] - val(R[0]);
+    double b = m.X[1][y] - val(R[1]);
     double s = a * a + b * b;
     if (m.dims == 3) {
-        double c = m.X[2][z] - R[2];
+        double c = m.X[2][z] - val(R[2]);
         s = s + c * c;
     }
     return s < r2;
@@ -125,7 +202,8 @@ inline bool in_sphere(const Model& m, int64_t x, int64_t y, int64_t z, const dou
 
 // per-axis index range that can satisfy the sphere test (conservative and
 // exact: fl(a*a) <= the full rounded sum, so nodes outside fail the test too)
-void axis_range(const Model& m, int a, double Ra, double r2, int64_t& lo, int64_t& hi) {
+template <class Real>
+void axis_range(const Model<Real>& m, int a, double Ra, double r2, int64_t& lo, int64_t& hi) {
     lo = m.n[a];
     hi = -1;
     for (int64_t i = 0; i < m.n[a]; ++i) {
@@ -137,11 +215,12 @@ void axis_range(const Model& m, int a, double Ra, double r2, int64_t& lo, int64_
     }
 }
 
-void get_sphere(const Model& m, double radius, const double* R, std::vector<uint8_t>& S) {
+template <class Real>
+void get_sphere(const Model<Real>& m, double radius, const Real* R, std::vector<uint8_t>& S) {
     S.assign(m.N, 0);
     double r2 = radius * radius;
     int64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    for (int a = 0; a < m.dims; ++a) axis_range(m, a, R[a], r2, lo[a], hi[a]);
+    for (int a = 0; a < m.dims; ++a) axis_range(m, a, val(R[a]), r2, lo[a], hi[a]);
     if (m.dims == 2) { lo[2] = 0; hi[2] = 0; }
     for (int64_t z = lo[2]; z <= hi[2]; ++z)
         for (int64_t y = lo[1]; y <= hi[1]; ++y)
@@ -151,22 +230,24 @@ void get_sphere(const Model& m, double radius, const double* R, std::vector<uint
 
 // dot of a vector with a lattice vector, vectorFieldDotVector (kernels.jl:198-224):
 // sumTerm = 0 then += v_k * c_k in component order
-inline double dot_c(const double* v, const std::array<int, 3>& c, int dims) {
-    double s = 0.0;
+template <class V>
+inline V dot_c(const V* v, const std::array<int, 3>& c, int dims) {
+    V s = 0.0;
     for (int k = 0; k < dims; ++k) s += v[k] * (double)c[k];
     return s;
 }
 
 // getNodeVelocity evaluated at node y (aux.jl:229-263, kernels.jl:376-415)
-void node_velocity(const Model& m, const Particle& p, int64_t y, double* out) {
+template <class Real>
+void node_velocity(const Model<Real>& m, const Particle<Real>& p, int64_t y, Real* out) {
     int d = m.dims;
-    double xr[3] = {0, 0, 0};
+    Real xr[3] = {0, 0, 0};
     for (int k = 0; k < d; ++k) xr[k] = m.coord(k, y) + (-p.nvR[k]);
-    double nrm2 = 0.0;
+    Real nrm2 = 0.0;
     for (int k = 0; k < d; ++k) nrm2 += xr[k] * xr[k];
-    double nrm = std::sqrt(nrm2);
+    Real nrm = sqrt(nrm2);
     if (nrm == 0) nrm = 1;
-    double bulk[3];
+    Real bulk[3];
     if (d == 2) {
         bulk[0] = p.nvV[0] - p.nvW[0] * xr[1];
         bulk[1] = p.nvV[1] + p.nvW[0] * xr[0];
@@ -179,19 +260,20 @@ void node_velocity(const Model& m, const Particle& p, int64_t y, double* out) {
         for (int k = 0; k < d; ++k) out[k] = bulk[k];
         return;
     }
-    double inv = 1.0 / nrm;
-    double ur[3];
+    Real inv = 1.0 / nrm;
+    Real ur[3];
     for (int k = 0; k < d; ++k) ur[k] = inv * xr[k];
-    double edr = 0.0;
+    Real edr = 0.0;
     for (int k = 0; k < d; ++k) edr += ur[k] * p.nvE[k];
-    double first = p.B1 + p.B2 * edr;
+    Real first = p.B1 + p.B2 * edr;
     for (int k = 0; k < d; ++k) {
-        double second = edr * ur[k] + (-p.nvE[k]);
+        Real second = edr * ur[k] + (-p.nvE[k]);
         out[k] = first * second + bulk[k];
     }
 }
 
-void capture_node_velocity(Particle& p) {
+template <class Real>
+void capture_node_velocity(Particle<Real>& p) {
     for (int k = 0; k < 3; ++k) {
         p.nvR[k] = p.R[k];
         p.nvV[k] = p.v[k];
@@ -202,91 +284,95 @@ void capture_node_velocity(Particle& p) {
 
 // hydroVariablesUpdate! (fluids.jl:7-37): rho = sum_i f_i ; rho*u = sum_i f_i c_i
 // (+ dt/2 F with Guo) ; u = rho*u / rho unless rho == 0 (isapprox with atol 0)
-void hydro(Model& m) {
+template <class Real>
+void hydro(Model<Real>& m) {
     const int64_t N = m.N;
     const int d = m.dims, Q = m.vs.q;
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < N; ++c) {
-        double r = 0.0;
+        Real r = 0.0;
         for (int i = 0; i < Q; ++i) r = (i == 0) ? m.f[c] : r + m.f[(int64_t)i * N + c];
         m.rho[c] = r;
         for (int k = 0; k < d; ++k) {
-            double j = 0.0;
+            Real j = 0.0;
             for (int i = 0; i < Q; ++i) {
-                double t = m.f[(int64_t)i * N + c] * (double)m.vs.c[i][k];
+                Real t = m.f[(int64_t)i * N + c] * (double)m.vs.c[i][k];
                 j = (i == 0) ? t : j + t;
             }
             if (m.guo) j = j + (0.5 * m.dt) * m.F[(int64_t)k * N + c];
-            m.u[(int64_t)k * N + c] = (r == 0.0) ? 0.0 : j / r;
+            m.u[(int64_t)k * N + c] = (r == 0.0) ? Real(0.0) : j / r;
         }
     }
 }
 
 // equilibriumDistribution (fluids.jl:39-52) at one cell
-inline double feq(const Model& m, int i, int64_t c) {
+template <class Real>
+inline Real feq(const Model<Real>& m, int i, int64_t c) {
     const int d = m.dims;
-    double uc = 0.0, uu = 0.0;
+    Real uc = 0.0, uu = 0.0;
     for (int k = 0; k < d; ++k) uc += m.u[(int64_t)k * m.N + c] * (double)m.vs.c[i][k];
     for (int k = 0; k < d; ++k) uu += m.u[(int64_t)k * m.N + c] * m.u[(int64_t)k * m.N + c];
-    double first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
-    double second = first - uu * (0.5 * m.invC2);
+    Real first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
+    Real second = first - uu * (0.5 * m.invC2);
     double wi = m.vs.w[i];
     if (m.compressible) return wi * ((second + 1) * m.rho[c]);
     return wi * m.rho[c] + wi * (m.rho0[c] * second);
 }
 
 // guoForcingTerm (fluids.jl:103-127) at one cell
-inline double guo(const Model& m, int i, int64_t c) {
+template <class Real>
+inline Real guo(const Model<Real>& m, int i, int64_t c) {
     const int d = m.dims;
     const auto& ci = m.vs.c[i];
-    double U[3] = {0, 0, 0}, Fv[3] = {0, 0, 0};
+    Real U[3] = {0, 0, 0}, Fv[3] = {0, 0, 0};
     for (int k = 0; k < d; ++k) {
         U[k] = m.u[(int64_t)k * m.N + c];
         Fv[k] = m.F[(int64_t)k * m.N + c];
     }
-    double uc = 0.0;
+    Real uc = 0.0;
     for (int k = 0; k < d; ++k) uc += U[k] * (double)ci[k];
     double wi = m.vs.w[i];
     if (!m.trt) {
-        double inter = 0.0;
+        Real inter = 0.0;
         for (int k = 0; k < d; ++k) {
-            double second = (uc * (double)ci[k]) * m.invC4;
-            double first = ((-U[k]) + (double)ci[k]) * m.invC2;
+            Real second = (uc * (double)ci[k]) * m.invC4;
+            Real first = ((-U[k]) + (double)ci[k]) * m.invC2;
             inter += (first + second) * Fv[k];
         }
         return wi * m.dt * (1 - m.dt / (2 * m.tau)) * inter;
     }
-    double inter = 0.0;
+    Real inter = 0.0;
     for (int k = 0; k < d; ++k) {
-        double second = (uc * (double)ci[k]) * m.invC4;
+        Real second = (uc * (double)ci[k]) * m.invC4;
         inter += ((-U[k]) * m.invC2 + second) * Fv[k];
     }
-    double plus = (1 - m.dt / (2 * m.tau_plus)) * inter;
-    double inter2 = 0.0;
+    Real plus = (1 - m.dt / (2 * m.tau_plus)) * inter;
+    Real inter2 = 0.0;
     for (int k = 0; k < d; ++k) inter2 += Fv[k] * ((double)ci[k] * m.invC2);
-    double minus = (1 - m.dt / (2 * m.tau_minus)) * inter2;
+    Real minus = (1 - m.dt / (2 * m.tau_minus)) * inter2;
     return wi * m.dt * (plus + minus);
 }
 
 // collisionStep (fluids.jl:58-101): returns f + Omega
-void collision(const Model& m, std::vector<double>& fs) {
+template <class Real>
+void collision(const Model<Real>& m, std::vector<Real>& fs) {
     const int64_t N = m.N;
     const int Q = m.vs.q;
     fs.resize((size_t)N * Q);
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < N; ++c) {
-        double eq[27];
+        Real eq[27];
         for (int i = 0; i < Q; ++i) eq[i] = feq(m, i, c);
         for (int i = 0; i < Q; ++i) {
-            double fi = m.f[(int64_t)i * N + c];
-            double om;
+            Real fi = m.f[(int64_t)i * N + c];
+            Real om;
             if (!m.trt) {
                 om = (-m.dt / m.tau) * (fi - eq[i]);
             } else {
                 int ib = m.vs.opp[i];
-                double fb = m.f[(int64_t)ib * N + c];
-                double fp = 0.5 * (fi + fb), fm = 0.5 * (fi - fb);
-                double ep = 0.5 * (eq[i] + eq[ib]), em = 0.5 * (eq[i] - eq[ib]);
+                Real fb = m.f[(int64_t)ib * N + c];
+                Real fp = 0.5 * (fi + fb), fm = 0.5 * (fi - fb);
+                Real ep = 0.5 * (eq[i] + eq[ib]), em = 0.5 * (eq[i] - eq[ib]);
                 om = (-m.dt / m.tau_plus) * (fp - ep) + (-m.dt / m.tau_minus) * (fm - em);
             }
             if (m.guo) om = om + guo(m, i, c);
@@ -296,14 +382,16 @@ void collision(const Model& m, std::vector<double>& fs) {
 }
 
 // streamingInvasionRegions[j](x) = S(x + c_j) && !S(x)   (aux.jl:190)
-inline bool invasion(const Model& m, const std::vector<uint8_t>& S, int j, int64_t c) {
+template <class Real>
+inline bool invasion(const Model<Real>& m, const std::vector<uint8_t>& S, int j, int64_t c) {
     if (S[c]) return false;
     const auto& cj = m.vs.c[j];
     return S[m.shifted(c, cj[0], cj[1], cj[2])] != 0;
 }
 
 // 2D/3D cross product of the reference (aux.jl:139-145)
-void cross_ref(int d, const double* v, const double* w, double* out) {
+template <class A, class B, class C>
+void cross_ref(int d, const A* v, const B* w, C* out) {
     if (d == 2) {
         out[0] = v[0] * w[1] - v[1] * w[0];
     } else {
@@ -314,7 +402,8 @@ void cross_ref(int d, const double* v, const double* w, double* out) {
 }
 
 // sorted fluid cells x with x - c_id in S and x not in S (conjugate boundary nodes)
-void particle_links(const Model& m, const Particle& p, int id, std::vector<int64_t>& out) {
+template <class Real>
+void particle_links(const Model<Real>& m, const Particle<Real>& p, int id, std::vector<int64_t>& out) {
     out.clear();
     const auto& ci = m.vs.c[id];
     if (ci[0] == 0 && ci[1] == 0 && ci[2] == 0) return;
@@ -327,12 +416,13 @@ void particle_links(const Model& m, const Particle& p, int id, std::vector<int64
 }
 
 // moveParticles! (particles.jl:7-92)
-void move_particle(Model& m, Particle& p, bool initial) {
+template <class Real>
+void move_particle(Model<Real>& m, Particle<Real>& p, bool initial) {
     const int d = m.dims;
     bool moved = initial, need_nv = initial;
     if (!initial) {
         if (p.couple_f) {
-            double A[3];
+            Real A[3];
             for (int k = 0; k < d; ++k) A[k] = p.F[k] * p.inv_mass;
             // the tick == 0 half step (particles.jl:19) is unreachable: tick! has
             // already incremented model.tick when it calls moveParticles!
@@ -343,42 +433,42 @@ void move_particle(Model& m, Particle& p, bool initial) {
         }
         if (p.couple_t) {
             int nw = d == 2 ? 1 : 3;
-            double Al[3];
+            Real Al[3];
             for (int k = 0; k < nw; ++k) Al[k] = p.T[k] * p.inv_inertia;
             for (int k = 0; k < nw; ++k) p.w[k] = p.w[k] + m.dt * Al[k];
             if (p.kind == LBM_SQUIRMER) {
-                double theta;
+                Real theta;
                 if (d == 2) {
-                    theta = std::fabs(p.w[0]);
+                    theta = fabs(p.w[0]);
                 } else {
-                    double s = 0.0;
+                    Real s = 0.0;
                     for (int k = 0; k < 3; ++k) s += p.w[k] * p.w[k];
-                    theta = std::sqrt(s);
+                    theta = sqrt(s);
                 }
                 if (theta != 0.0) {  // !(theta ≈ 0) with atol 0
-                    double vr[3] = {0, 0, 0};
-                    const double* v = p.e;
+                    Real vr[3] = {0, 0, 0};
+                    const Real* v = p.e;
                     if (d == 2) {
-                        double k = p.w[0] / theta;
+                        Real k = p.w[0] / theta;
                         theta = theta * m.dt;
-                        double cr[2] = {-k * v[1], k * v[0]};
-                        double ct = std::cos(theta), st = std::sin(theta);
+                        Real cr[2] = {-k * v[1], k * v[0]};
+                        Real ct = cos(theta), st = sin(theta);
                         for (int q = 0; q < 2; ++q) vr[q] = v[q] * ct + cr[q] * st;
                     } else {
-                        double k[3];
+                        Real k[3];
                         for (int q = 0; q < 3; ++q) k[q] = p.w[q] / theta;
                         theta = theta * m.dt;
-                        double cr[3];
+                        Real cr[3];
                         cross_ref(3, k, v, cr);
-                        double ct = std::cos(theta), st = std::sin(theta);
+                        Real ct = cos(theta), st = sin(theta);
                         for (int q = 0; q < 3; ++q) vr[q] = v[q] * ct + cr[q] * st;
-                        double kv = 0.0;
+                        Real kv = 0.0;
                         for (int q = 0; q < 3; ++q) kv += k[q] * v[q];
                         for (int q = 0; q < 3; ++q) vr[q] = vr[q] + k[q] * kv * (1 - ct);
                     }
-                    double s = 0.0;
+                    Real s = 0.0;
                     for (int q = 0; q < d; ++q) s += vr[q] * vr[q];
-                    double nr = std::sqrt(s);
+                    Real nr = sqrt(s);
                     for (int q = 0; q < d; ++q) p.e[q] = vr[q] / nr;
                 }
             }
@@ -397,7 +487,8 @@ void move_particle(Model& m, Particle& p, bool initial) {
     if (need_nv) capture_node_velocity(p);
 }
 
-void tick(Model& m, std::vector<double>& fs, std::vector<double>& fn) {
+template <class Real>
+void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
     const int64_t N = m.N;
     const int Q = m.vs.q, d = m.dims;
     collision(m, fs);
@@ -408,13 +499,13 @@ void tick(Model& m, std::vector<double>& fs, std::vector<double>& fn) {
         const auto& ci = m.vs.c[id];
         const int ib = m.vs.opp[id];
         const double wi = m.vs.w[id];
-        double* s = &fn[(size_t)id * N];
-        const double* fsi = &fs[(size_t)id * N];
-        const double* fsb = &fs[(size_t)ib * N];
+        Real* s = &fn[(size_t)id * N];
+        const Real* fsi = &fs[(size_t)id * N];
+        const Real* fsb = &fs[(size_t)ib * N];
 #pragma omp parallel for schedule(static)
         for (int64_t c = 0; c < N; ++c) {
             // circshift (pull): out(x) = in(x - c)
-            double v = fsi[m.shifted(c, -ci[0], -ci[1], -ci[2])];
+            Real v = fsi[m.shifted(c, -ci[0], -ci[1], -ci[2])];
             if (m.bounce_back) {
                 if (m.W[c]) v = 0;
                 bool region = invasion(m, m.W, ib, c);
@@ -438,24 +529,24 @@ void tick(Model& m, std::vector<double>& fs, std::vector<double>& fn) {
                 if (nodes.empty()) break;  // fluids.jl:184 exits the particle loop
                 for (int64_t x : nodes) {
                     int64_t src = m.shifted(x, -ci[0], -ci[1], -ci[2]);
-                    double up[3];
+                    Real up[3];
                     node_velocity(m, p, src, up);
                     s[x] += (2 * wi * m.invC2) * m.rho[x] * dot_c(up, ci, d);
                 }
                 if (p.couple_f || p.couple_t) {
                     if (p.couple_f) {
-                        double S = 0.0;
+                        Real S = 0.0;
                         for (int64_t x : nodes) S += fsb[x] + s[x];
                         for (int k = 0; k < d; ++k) p.F[k] -= coeff * S * (double)ci[k];
                     }
                     if (p.couple_t) {
-                        double aux[3] = {0, 0, 0};
+                        Real aux[3] = {0, 0, 0};
                         for (int64_t x : nodes) {
-                            double st = fsb[x] + s[x];
+                            Real st = fsb[x] + s[x];
                             for (int k = 0; k < d; ++k) aux[k] += st * (m.coord(k, x) + (-p.R[k]));
                         }
                         double cd[3] = {(double)ci[0], (double)ci[1], (double)ci[2]};
-                        double cr[3] = {0, 0, 0};
+                        Real cr[3] = {0, 0, 0};
                         cross_ref(d, aux, cd, cr);
                         int nt = d == 2 ? 1 : 3;
                         for (int k = 0; k < nt; ++k) p.T[k] -= coeff * cr[k];
@@ -472,37 +563,32 @@ void tick(Model& m, std::vector<double>& fs, std::vector<double>& fn) {
         for (auto& p : m.parts) move_particle(m, p, false);
 }
 
-struct Handle {
-    Model m;
-    std::vector<double> fs, fn;
+template <class Real>
+struct HandleT {
+    Model<Real> m;
+    std::vector<Real> fs, fn;
 };
+using Handle = HandleT<double>;
+using DualHandle = HandleT<D6>;
 
-}  // namespace
-
-extern "C" {
-
-const char* orc_last_error(void) { return g_err.c_str(); }
-
-void orc_set_threads(int n) {
-#ifdef _OPENMP
-    if (n > 0) omp_set_num_threads(n);
-#else
-    (void)n;
-#endif
+// seed: value `x` with derivatives `dx[kDirs]` (null: none); plain for double
+inline double seeded(double x, const double*) { return x; }
+inline D6 seeded_d(double x, const double* dx) {
+    D6 r(x);
+    if (dx)
+        for (int k = 0; k < kDirs; ++k) r.d[k] = dx[k];
+    return r;
 }
+template <class Real> Real seed_as(double x, const double* dx);
+template <> double seed_as<double>(double x, const double* dx) { return seeded(x, dx); }
+template <> D6 seed_as<D6>(double x, const double* dx) { return seeded_d(x, dx); }
 
-int orc_max_threads(void) {
-#ifdef _OPENMP
-    return omp_get_max_threads();
-#else
-    return 1;
-#endif
-}
-
-int orc_create(const lbm_config* cfg, void** out) {
-    if (!cfg || !out) return fail(LBM_ERR_INVALID, "null argument");
-    auto h = std::make_unique<Handle>();
-    Model& m = h->m;
+// modelInit + findInitialConditions into m.  seeds (dual model only):
+// derivatives of tau+ (and the BGK tau), tau- and of each uniform force
+// component along the kDirs directions.
+template <class Real>
+int create_model(const lbm_config* cfg, Model<Real>& m, const double* seed_tau_plus, const double* seed_tau_minus,
+                 const double* seed_force) {
     if (cfg->dims != 2 && cfg->dims != 3) return fail(LBM_ERR_INVALID, "dims must be 2 or 3");
     m.dims = cfg->dims;
     m.vs = make_velocity_set(cfg->lattice);
@@ -523,10 +609,10 @@ int orc_create(const lbm_config* cfg, void** out) {
     if (cfg->collision != LBM_BGK && cfg->collision != LBM_TRT)
         return fail(LBM_ERR_INVALID, "Collision model is not implemented!");
     m.trt = cfg->collision == LBM_TRT;
-    m.tau = cfg->tau;
-    m.tau_plus = cfg->tau;
-    m.tau_minus = cfg->tau_minus;
-    if (!(m.tau > 0) || (m.trt && !(m.tau_minus > 0))) return fail(LBM_ERR_INVALID, "relaxation times must be positive");
+    m.tau = seed_as<Real>(cfg->tau, seed_tau_plus);
+    m.tau_plus = seed_as<Real>(cfg->tau, seed_tau_plus);
+    m.tau_minus = seed_as<Real>(cfg->tau_minus, seed_tau_minus);
+    if (!(cfg->tau > 0) || (m.trt && !(cfg->tau_minus > 0))) return fail(LBM_ERR_INVALID, "relaxation times must be positive");
     m.compressible = cfg->compressible != 0;
     const int64_t N = m.N;
     const int d = m.dims, Q = m.vs.q;
@@ -564,10 +650,13 @@ int orc_create(const lbm_config* cfg, void** out) {
     if (cfg->force_mode == LBM_FORCE_UNIFORM || cfg->force_mode == LBM_FORCE_FIELD) {
         if (cfg->force_mode == LBM_FORCE_FIELD && !cfg->force_field)
             return fail(LBM_ERR_INVALID, "force density does not have consistent dimensions!");
-        for (int k = 0; k < d; ++k)
+        for (int k = 0; k < d; ++k) {
+            const Real Fk = seed_as<Real>(cfg->force_mode == LBM_FORCE_UNIFORM ? cfg->force[k] : 0.0,
+                                          seed_force ? seed_force + (size_t)k * kDirs : nullptr);
             for (int64_t c = 0; c < N; ++c)
-                m.F[(int64_t)k * N + c] = m.W[c] ? 0.0
-                    : (cfg->force_mode == LBM_FORCE_UNIFORM ? cfg->force[k] : cfg->force_field[(int64_t)k * N + c]);
+                m.F[(int64_t)k * N + c] = m.W[c] ? Real(0.0)
+                    : (cfg->force_mode == LBM_FORCE_UNIFORM ? Fk : Real(cfg->force_field[(int64_t)k * N + c]));
+        }
         m.guo = true;
     } else if (cfg->force_mode != LBM_FORCE_NONE) {
         return fail(LBM_ERR_INVALID, "unknown force mode");
@@ -576,37 +665,37 @@ int orc_create(const lbm_config* cfg, void** out) {
     // findInitialConditions (initMethods.jl:417-438)
     m.f.assign((size_t)N * Q, 0.0);
     for (int64_t c = 0; c < N; ++c) {
-        double uu_[3] = {0, 0, 0};
+        Real uu_[3] = {0, 0, 0};
         for (int k = 0; k < d; ++k) {
-            double uk = m.u[(int64_t)k * N + c];
+            Real uk = m.u[(int64_t)k * N + c];
             if (m.guo) {
-                double cons = (m.rho[c] == 0.0) ? 0.0 : m.F[(int64_t)k * N + c] / m.rho[c];
+                Real cons = (m.rho[c] == 0.0) ? Real(0.0) : m.F[(int64_t)k * N + c] / m.rho[c];
                 uk = uk - 0.5 * m.dt * cons;
             }
             uu_[k] = uk;
         }
         for (int i = 0; i < Q; ++i) {
-            double uc = dot_c(uu_, m.vs.c[i], d);
-            double first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
-            double uu = 0.0;
+            Real uc = dot_c(uu_, m.vs.c[i], d);
+            Real first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
+            Real uu = 0.0;
             for (int k = 0; k < d; ++k) uu += uu_[k] * uu_[k];
-            double second = first - uu * (0.5 * m.invC2) + 1;
+            Real second = first - uu * (0.5 * m.invC2) + 1;
             m.f[(int64_t)i * N + c] = second * (m.vs.w[i] * m.rho[c]);
         }
     }
     hydro(m);
-    *out = h.release();
     return LBM_OK;
 }
 
-int orc_add_particle(void* hp, const lbm_particle_params* pp, int32_t* id_out) {
-    if (!hp || !pp) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+// addBead!/addSquirmer! into m (seeds: derivatives of B1 and B2, dual model only)
+template <class Real>
+int add_particle(Model<Real>& m, const lbm_particle_params* pp, const double* seed_B1, const double* seed_B2,
+                 int32_t* id_out) {
     if (pp->kind != LBM_BEAD && pp->kind != LBM_SQUIRMER) return fail(LBM_ERR_INVALID, "unknown particle kind");
     if (m.parts.size() >= 255) return fail(LBM_ERR_INVALID, "particle ids are UInt8: at most 255 particles");
     if (!(pp->radius > 0)) return fail(LBM_ERR_INVALID, "radius must be positive");
     const int d = m.dims;
-    Particle p;
+    Particle<Real> p;
     p.id = (int)m.parts.size() + 1;
     p.kind = pp->kind;
     p.couple_f = pp->couple_forces != 0;
@@ -614,7 +703,7 @@ int orc_add_particle(void* hp, const lbm_particle_params* pp, int32_t* id_out) {
     p.radius = pp->radius;
     // mass: origin-centred sphere node count (initMethods.jl:108)
     std::vector<uint8_t> S0;
-    double zero[3] = {0, 0, 0};
+    Real zero[3] = {0, 0, 0};
     get_sphere(m, pp->radius, zero, S0);
     int64_t count = 0;
     for (uint8_t s : S0) count += s;
@@ -630,8 +719,8 @@ int orc_add_particle(void* hp, const lbm_particle_params* pp, int32_t* id_out) {
     if (d == 2) p.w[0] = pp->angular_velocity[0];
     else for (int k = 0; k < 3; ++k) p.w[k] = pp->angular_velocity[k];
     if (p.kind == LBM_SQUIRMER) {
-        p.B1 = pp->B1;
-        p.B2 = pp->B2;
+        p.B1 = seed_as<Real>(pp->B1, seed_B1);
+        p.B2 = seed_as<Real>(pp->B2, seed_B2);
         for (int k = 0; k < d; ++k) p.e[k] = pp->swimming_direction[k];
     }
     m.parts.push_back(p);
@@ -640,6 +729,42 @@ int orc_add_particle(void* hp, const lbm_particle_params* pp, int32_t* id_out) {
     move_particle(m, m.parts.back(), true);
     if (id_out) *id_out = m.parts.back().id;
     return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int orc_create(const lbm_config* cfg, void** out) {
+    if (!cfg || !out) return fail(LBM_ERR_INVALID, "null argument");
+    auto h = std::make_unique<Handle>();
+    const int rc = create_model(cfg, h->m, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    *out = h.release();
+    return LBM_OK;
+}
+
+int orc_add_particle(void* hp, const lbm_particle_params* pp, int32_t* id_out) {
+    if (!hp || !pp) return fail(LBM_ERR_INVALID, "null argument");
+    return add_particle(static_cast<Handle*>(hp)->m, pp, nullptr, nullptr, id_out);
 }
 
 int orc_step(void* hp, int64_t n) {
@@ -652,7 +777,7 @@ int orc_step(void* hp, int64_t n) {
 
 int orc_get_fields(void* hp, double* rho, double* u) {
     if (!hp) return fail(LBM_ERR_INVALID, "null handle");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     if (rho) std::copy(m.rho.begin(), m.rho.end(), rho);
     if (u) std::copy(m.u.begin(), m.u.end(), u);
     return LBM_OK;
@@ -660,14 +785,14 @@ int orc_get_fields(void* hp, double* rho, double* u) {
 
 int orc_get_distributions(void* hp, double* f) {
     if (!hp || !f) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     std::copy(m.f.begin(), m.f.end(), f);
     return LBM_OK;
 }
 
 int orc_set_distributions(void* hp, const double* f) {
     if (!hp || !f) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     std::copy(f, f + m.f.size(), m.f.begin());
     hydro(m);
     return LBM_OK;
@@ -675,10 +800,10 @@ int orc_set_distributions(void* hp, const double* f) {
 
 int orc_get_particles(void* hp, lbm_particle_state* out, int32_t cap, int32_t* count) {
     if (!hp) return fail(LBM_ERR_INVALID, "null handle");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     if (count) *count = (int32_t)m.parts.size();
     for (int32_t i = 0; i < cap && i < (int32_t)m.parts.size(); ++i) {
-        const Particle& p = m.parts[i];
+        const Particle<double>& p = m.parts[i];
         lbm_particle_state& s = out[i];
         std::memset(&s, 0, sizeof(s));
         s.id = p.id;
@@ -704,7 +829,7 @@ int orc_get_particles(void* hp, lbm_particle_state* out, int32_t cap, int32_t* c
 
 int orc_get_mask(void* hp, int32_t id, uint8_t* mask) {
     if (!hp || !mask) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
     std::copy(m.parts[id - 1].S.begin(), m.parts[id - 1].S.end(), mask);
     return LBM_OK;
@@ -712,7 +837,7 @@ int orc_get_mask(void* hp, int32_t id, uint8_t* mask) {
 
 int orc_get_links(void* hp, int32_t id, int64_t* cells, int8_t* dirs, int64_t cap, int64_t* n) {
     if (!hp || !n) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
     std::vector<int64_t> nodes;
     int64_t k = 0;
@@ -732,7 +857,7 @@ int orc_get_links(void* hp, int32_t id, int64_t* cells, int8_t* dirs, int64_t ca
 
 int orc_get_info(void* hp, lbm_info* info) {
     if (!hp || !info) return fail(LBM_ERR_INVALID, "null argument");
-    Model& m = static_cast<Handle*>(hp)->m;
+    Model<double>& m = static_cast<Handle*>(hp)->m;
     std::memset(info, 0, sizeof(*info));
     info->dims = m.dims;
     info->lattice = m.vs.q;
@@ -760,5 +885,61 @@ int orc_velocity_set(int32_t q, int8_t* c, double* w, int32_t* opp) {
 }
 
 void orc_destroy(void* hp) { delete static_cast<Handle*>(hp); }
+
+// ---- dual-number oracle: derivatives along kDirs seeded directions ---------
+int ord_directions(void) { return kDirs; }
+
+// seed_tau_plus / seed_tau_minus: [kDirs]; seed_force: [3][kDirs] (uniform force); any may be null
+int ord_create(const lbm_config* cfg, const double* seed_tau_plus, const double* seed_tau_minus,
+               const double* seed_force, void** out) {
+    if (!cfg || !out) return fail(LBM_ERR_INVALID, "null argument");
+    auto h = std::make_unique<DualHandle>();
+    const int rc = create_model(cfg, h->m, seed_tau_plus, seed_tau_minus, seed_force);
+    if (rc) return rc;
+    *out = h.release();
+    return LBM_OK;
+}
+
+int ord_add_particle(void* hp, const lbm_particle_params* pp, const double* seed_B1, const double* seed_B2,
+                     int32_t* id_out) {
+    if (!hp || !pp) return fail(LBM_ERR_INVALID, "null argument");
+    return add_particle(static_cast<DualHandle*>(hp)->m, pp, seed_B1, seed_B2, id_out);
+}
+
+int ord_step(void* hp, int64_t n) {
+    if (!hp) return fail(LBM_ERR_INVALID, "null handle");
+    if (n < 0) return fail(LBM_ERR_INVALID, "ticks must be non-negative");
+    auto* h = static_cast<DualHandle*>(hp);
+    for (int64_t t = 0; t < n; ++t) tick(h->m, h->fs, h->fn);
+    return LBM_OK;
+}
+
+// particle `id` (1-based): values [12] = position, velocity, angular velocity,
+// swimming direction (3 each); derivatives [12][kDirs] in the same order
+int ord_particle(void* hp, int32_t id, double* values, double* derivs) {
+    if (!hp || !values || !derivs) return fail(LBM_ERR_INVALID, "null argument");
+    const Model<D6>& m = static_cast<DualHandle*>(hp)->m;
+    if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
+    const Particle<D6>& p = m.parts[id - 1];
+    const D6* groups[4] = {p.R, p.v, p.w, p.e};
+    for (int g = 0; g < 4; ++g)
+        for (int k = 0; k < 3; ++k) {
+            const D6& x = groups[g][k];
+            values[3 * g + k] = x.v;
+            for (int q = 0; q < kDirs; ++q) derivs[(size_t)(3 * g + k) * kDirs + q] = x.d[q];
+        }
+    return LBM_OK;
+}
+
+// density and velocity values (as orc_get_fields)
+int ord_get_fields(void* hp, double* rho, double* u) {
+    if (!hp) return fail(LBM_ERR_INVALID, "null handle");
+    const Model<D6>& m = static_cast<DualHandle*>(hp)->m;
+    for (size_t c = 0; rho && c < m.rho.size(); ++c) rho[c] = m.rho[c].v;
+    for (size_t c = 0; u && c < m.u.size(); ++c) u[c] = m.u[c].v;
+    return LBM_OK;
+}
+
+void ord_destroy(void* hp) { delete static_cast<DualHandle*>(hp); }
 
 }  // extern "C"

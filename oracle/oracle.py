@@ -62,6 +62,13 @@ def load() -> C.CDLL:
     lib.orc_get_info.argtypes = [vp, C.POINTER(capi.LbmInfo)]
     lib.orc_velocity_set.argtypes = [C.c_int32, C.POINTER(C.c_int8), dp, C.POINTER(C.c_int32)]
     lib.orc_destroy.argtypes = [vp]
+    lib.ord_directions.restype = C.c_int
+    lib.ord_create.argtypes = [C.POINTER(capi.LbmConfig), dp, dp, dp, C.POINTER(vp)]
+    lib.ord_add_particle.argtypes = [vp, C.POINTER(capi.LbmParticleParams), dp, dp, C.POINTER(C.c_int32)]
+    lib.ord_step.argtypes = [vp, C.c_int64]
+    lib.ord_particle.argtypes = [vp, C.c_int32, dp, dp]
+    lib.ord_get_fields.argtypes = [vp, dp, dp]
+    lib.ord_destroy.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -155,6 +162,76 @@ class OracleModel:
     def close(self):
         if self.h:
             self.lib.orc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# derivative directions of the dual-number oracle
+DIRECTIONS = ("B1", "B2", "tau", "Fx", "Fy", "Fz")
+
+
+def tau_minus_slope(resolved) -> float:
+    """d tau- / d tau+ at fixed magic parameter: tau- = L dt^2 / (tau+ - dt/2) + dt/2 (TRT), 0 for BGK."""
+    if resolved.collision != "trt":
+        return 0.0
+    lam = resolved.kineticParameter
+    if isinstance(lam, str):
+        raise ValueError("the dual oracle needs a numeric kineticParameter")
+    dt = resolved.dt
+    return -float(lam) * dt * dt / (resolved.tau - dt / 2) ** 2
+
+
+class DualOracle:
+    """The oracle with forward-mode dual numbers: every quantity carries its
+    derivatives along DIRECTIONS (B1 and B2 of the particles added, the
+    relaxation time tau+ with tau- following at fixed magic parameter, and the
+    three components of the uniform body force).  Values equal the FP64
+    oracle's; solid masks are taken as computed (comparisons see values)."""
+
+    def __init__(self, resolved):
+        self.lib = load()
+        K = int(self.lib.ord_directions())
+        assert K == len(DIRECTIONS)
+        self.K = K
+        e = np.eye(K)
+        tp = np.ascontiguousarray(e[2])
+        tm = np.ascontiguousarray(e[2] * tau_minus_slope(resolved))
+        fs = np.ascontiguousarray(e[3:6])
+        self._seeds = (tp, tm, fs)
+        self.h = C.c_void_p()
+        dp = capi._dp
+        _check(self.lib.ord_create(C.byref(resolved.cfg), tp.ctypes.data_as(dp), tm.ctypes.data_as(dp),
+                                   fs.ctypes.data_as(dp), C.byref(self.h)))
+
+    def add_particle(self, params) -> int:
+        e = np.eye(self.K)
+        b1, b2 = np.ascontiguousarray(e[0]), np.ascontiguousarray(e[1])
+        pid = C.c_int32()
+        _check(self.lib.ord_add_particle(self.h, C.byref(params), b1.ctypes.data_as(capi._dp),
+                                         b2.ctypes.data_as(capi._dp), C.byref(pid)))
+        return pid.value
+
+    def step(self, n: int) -> None:
+        _check(self.lib.ord_step(self.h, int(n)))
+
+    def particle(self, pid: int = 1):
+        """(values, derivatives): dicts of position, velocity, angular_velocity,
+        swimming_direction -> (3,) values and (3, K) derivatives."""
+        v = np.zeros(12)
+        d = np.zeros((12, self.K))
+        _check(self.lib.ord_particle(self.h, pid, v.ctypes.data_as(capi._dp), d.ctypes.data_as(capi._dp)))
+        names = ("position", "velocity", "angular_velocity", "swimming_direction")
+        return ({n: v[3 * i:3 * i + 3] for i, n in enumerate(names)},
+                {n: d[3 * i:3 * i + 3] for i, n in enumerate(names)})
+
+    def close(self):
+        if self.h:
+            self.lib.ord_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
