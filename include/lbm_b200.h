@@ -297,6 +297,44 @@ int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out);
 const char* lbm_batch_last_error(const lbm_batch* b);
 void lbm_batch_destroy(lbm_batch* b);
 
+/* ---- gradients: discrete adjoint with binomial checkpointing --------------
+ * Observable: the time average, over ticks window_begin..window_end (after
+ * that many ticks, 1-based, inclusive), of the particle's velocity along
+ * `direction` (zero vector: its initial swimming direction), over a run of
+ * `ticks` ticks from the handle's initial state (tick 0).  Returns its value
+ * and its derivatives with respect to the particle's B1 and B2, the
+ * relaxation time tau (tau+ with tau- following: dtau = dtau_plus +
+ * tau_minus_slope * dtau_minus, the slope d tau-/d tau+ at fixed magic
+ * parameter being given by the caller) and the three components of the
+ * uniform body force.  The backward sweep runs a hand-written adjoint of the
+ * tick (stream-collide, bounce-back and moving-boundary links, momentum
+ * exchange) and of the particle update, recomputing forward segments from at
+ * most `snapshots` stored states (binomial checkpointing).  The solid masks
+ * are taken as the forward run computes them.  The handle is left in the
+ * state it had on entry.  Requirements: one particle, no walls, no per-node
+ * force field.  No counterpart in the reference (it has no differentiation). */
+typedef struct lbm_adjoint_spec {
+    int64_t ticks;
+    int64_t window_begin, window_end;
+    double direction[3];
+    double tau_minus_slope;
+    int32_t snapshots;    /* stored states, including the initial one (>= 2) */
+    int32_t reserved;
+} lbm_adjoint_spec;
+
+typedef struct lbm_adjoint_result {
+    double value;         /* the observable */
+    double dB1, dB2;
+    double dtau, dtau_plus, dtau_minus;
+    double dF[3];
+    int64_t forward_ticks;   /* ticks run forward in total (sweep and recomputation) */
+    int32_t snapshots_used;  /* most states held at once */
+    int32_t reserved;
+    double ms;               /* wall time of the call */
+} lbm_adjoint_result;
+
+int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result* out);
+
 /* Allocation-free stepping.  No counterpart in the reference.
  *
  * Same ticks and results as lbm_step, for callers that must not allocate

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -2156,5 +2157,410 @@ int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out) {
 const char* lbm_batch_last_error(const lbm_batch* b) { return b ? b->err.c_str() : g_global_err.c_str(); }
 
 void lbm_batch_destroy(lbm_batch* b) { batch_destroy_all(b); }
+
+}  // extern "C"
+
+// ===========================================================================
+// Gradients (lbm_adjoint): discrete adjoint of the tick with binomial
+// checkpointing.  Device: the field adjoint (adjoint.cuh).  Host: the
+// particle update's adjoint (a handful of FP64 values per tick) and the
+// checkpoint schedule.
+// ===========================================================================
+namespace {
+
+// forward-mode dual with one direction, host side
+struct HD {
+    double v = 0, d = 0;
+};
+HD operator+(HD a, HD b) { return {a.v + b.v, a.d + b.d}; }
+HD operator-(HD a, HD b) { return {a.v - b.v, a.d - b.d}; }
+HD operator*(HD a, HD b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+HD operator/(HD a, HD b) {
+    const double q = a.v / b.v;
+    return {q, (a.d - q * b.d) / b.v};
+}
+HD operator*(double s, HD a) { return {s * a.v, s * a.d}; }
+HD hsqrt(HD a) {
+    const double r = std::sqrt(a.v);
+    return {r, a.d / (2 * r)};
+}
+HD hcos(HD a) { return {std::cos(a.v), -std::sin(a.v) * a.d}; }
+HD hsin(HD a) { return {std::sin(a.v), std::cos(a.v) * a.d}; }
+HD habs(HD a) { return a.v < 0 ? HD{-a.v, -a.d} : a; }
+
+// the swimming-direction update of moveParticles! (particles.jl:48-70:
+// Rodrigues rotation by |w| dt about w, then normalised), as the particle
+// kernel does it
+void rodrigues(const HD* e, const HD* w, double dt, int D, HD* out) {
+    for (int k = 0; k < 3; ++k) out[k] = e[k];
+    HD theta;
+    if (D == 2) theta = habs(w[0]);
+    else theta = hsqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    if (theta.v == 0.0) return;
+    HD vr[3];
+    if (D == 2) {
+        const HD k = w[0] / theta;
+        const HD th = dt * theta;
+        const HD ct = hcos(th), st = hsin(th);
+        vr[0] = e[0] * ct + (HD{0, 0} - k * e[1]) * st;
+        vr[1] = e[1] * ct + (k * e[0]) * st;
+        vr[2] = HD{};
+    } else {
+        const HD k[3] = {w[0] / theta, w[1] / theta, w[2] / theta};
+        const HD th = dt * theta;
+        const HD ct = hcos(th), st = hsin(th);
+        const HD cr[3] = {k[1] * e[2] - k[2] * e[1], HD{0, 0} - k[0] * e[2] + k[2] * e[0], k[0] * e[1] - k[1] * e[0]};
+        const HD kv = k[0] * e[0] + k[1] * e[1] + k[2] * e[2];
+        for (int q = 0; q < 3; ++q) vr[q] = e[q] * ct + cr[q] * st + k[q] * kv * (HD{1, 0} - ct);
+    }
+    HD n2{};
+    for (int q = 0; q < D; ++q) n2 = n2 + vr[q] * vr[q];
+    const HD nr = hsqrt(n2);
+    for (int q = 0; q < D; ++q) out[q] = vr[q] / nr;
+}
+
+// adjoint of the particle state carried backwards through the ticks
+struct PartAdj {
+    double R[3] = {0, 0, 0}, v[3] = {0, 0, 0}, w[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+    double S[12] = {0};  // snapshot sR, sV, sW, sE
+    double mR[3] = {0, 0, 0};
+};
+
+struct Snap {
+    char* buf = nullptr;
+    long long tick = 0;
+    double time = 0;
+    int cur = 0;
+};
+
+struct AdjointRun {
+    lbm_handle* h = nullptr;
+    lbm_adjoint_spec spec{};
+    std::vector<ParticleDev> rec;  // rec[t]: the particle after t ticks
+    std::vector<char> have;        // rec[t] has been recorded
+    std::vector<Snap> snaps;       // stored states (a stack)
+    size_t snap_bytes = 0;
+    int max_used = 0;
+    long long forward = 0;
+    double* lam[2] = {nullptr, nullptr};
+    int lcur = 0;  // lam[lcur]: adjoint of the populations at the current tick
+    double* partial = nullptr;
+    double* dsum = nullptr;
+    long long nblocks = 0;
+    PartAdj pa;
+    double e0[3] = {0, 0, 0};
+    double dB1 = 0, dB2 = 0, dtp = 0, dtm = 0, dF[3] = {0, 0, 0};
+};
+
+std::vector<std::pair<void*, size_t>> snap_regions(lbm_handle* h) {
+    const size_t np = h->hparts.size();
+    return {{h->pop[h->cur], (size_t)h->N * h->q * storage_bytes(h->storage)},
+            {h->d_parts, sizeof(ParticleDev) * np},
+            {h->d_ivl, sizeof(int2) * h->ivl_slots},
+            {h->d_links, sizeof(int2) * h->link_slots},
+            {h->d_tilebits, sizeof(unsigned long long) * h->g.ntiles * h->words},
+            {h->d_nbox[0], sizeof(int) * 6 * np},
+            {h->d_nbox[1], sizeof(int) * 6 * np}};
+}
+
+int snap_push(AdjointRun& R) {
+    lbm_handle* h = R.h;
+    Snap s;
+    int rc = dev_alloc(h, &s.buf, R.snap_bytes);
+    if (rc) return rc;
+    char* p = s.buf;
+    for (auto& r : snap_regions(h)) {
+        if (r.first && r.second) CUDA_TRY(h, cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToDevice, h->stream));
+        p += r.second;
+    }
+    s.tick = h->tick;
+    s.time = h->time;
+    s.cur = h->cur;
+    R.snaps.push_back(s);
+    R.max_used = std::max(R.max_used, (int)R.snaps.size());
+    return LBM_OK;
+}
+
+int snap_restore(AdjointRun& R, const Snap& s) {
+    lbm_handle* h = R.h;
+    h->cur = s.cur;
+    h->tick = s.tick;
+    h->time = s.time;
+    h->part_pending = false;
+    char* p = s.buf;
+    for (auto& r : snap_regions(h)) {
+        if (r.first && r.second) CUDA_TRY(h, cudaMemcpyAsync(r.first, p, r.second, cudaMemcpyDeviceToDevice, h->stream));
+        p += r.second;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+void snap_pop(AdjointRun& R) {
+    dev_free(R.snaps.back().buf);
+    R.h->device_bytes -= R.snap_bytes;
+    R.snaps.pop_back();
+}
+
+// k ticks forward, recording the particle after each
+int advance(AdjointRun& R, long long k) {
+    lbm_handle* h = R.h;
+    for (long long s = 0; s < k; ++s) {
+        int rc = lbm_step(h, 1);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaMemcpy(&R.rec[h->tick], h->d_parts, sizeof(ParticleDev), cudaMemcpyDeviceToHost));
+        R.have[h->tick] = 1;
+        ++R.forward;
+    }
+    return LBM_OK;
+}
+
+// backward step of tick n; the device holds the state at tick n and
+// rec[n + 1] is known
+int backward_tick(AdjointRun& R, long long n) {
+    lbm_handle* h = R.h;
+    const int D = h->dims;
+    const ParticleDev& P0 = R.rec[n];
+    const ParticleDev& P1 = R.rec[n + 1];
+    PartAdj& A = R.pa;
+    const double dt = h->dt;
+    // the observable reads the velocity after tick n + 1
+    if (n + 1 >= R.spec.window_begin && n + 1 <= R.spec.window_end) {
+        const double K = (double)(R.spec.window_end - R.spec.window_begin + 1);
+        for (int k = 0; k < D; ++k) A.v[k] += R.e0[k] / K;
+    }
+    // reverse the particle update of tick n (particles.cuh, moveParticles!)
+    bool moved = false, alpha = false;
+    if (P0.coupleF)
+        for (int k = 0; k < D; ++k) moved = moved || P1.v[k] != 0.0;
+    if (P0.coupleT)
+        for (int k = 0; k < (D == 2 ? 1 : 3); ++k) alpha = alpha || P1.lastT[k] * P0.inv_inertia != 0.0;
+    if (moved || alpha) {  // the snapshot after the update is the updated state
+        for (int k = 0; k < 3; ++k) {
+            A.R[k] += A.S[k];
+            A.v[k] += A.S[3 + k];
+            A.w[k] += A.S[6 + k];
+            A.e[k] += A.S[9 + k];
+        }
+        for (double& s : A.S) s = 0.0;
+    }
+    if (moved) {  // the torque arm after the update is the new position
+        for (int k = 0; k < 3; ++k) A.R[k] += A.mR[k];
+        for (double& s : A.mR) s = 0.0;
+    }
+    if (P0.coupleT && P0.kind == LBM_SQUIRMER) {  // e' = rot(e, w')
+        double le[3] = {0, 0, 0}, lw[3] = {0, 0, 0};
+        for (int q = 0; q < 6; ++q) {
+            HD e[3], w[3], o[3];
+            for (int k = 0; k < 3; ++k) {
+                e[k] = HD{P0.e[k], q == k ? 1.0 : 0.0};
+                w[k] = HD{P1.w[k], q == 3 + k ? 1.0 : 0.0};
+            }
+            rodrigues(e, w, dt, D, o);
+            double g = 0.0;
+            for (int k = 0; k < D; ++k) g += A.e[k] * o[k].d;
+            if (q < 3) le[q] = g;
+            else lw[q - 3] = g;
+        }
+        for (int k = 0; k < 3; ++k) {
+            A.e[k] = le[k];
+            A.w[k] += lw[k];
+        }
+    }
+    AdjArgs a{};
+    if (P0.coupleT)
+        for (int k = 0; k < (D == 2 ? 1 : 3); ++k) a.lamT[k] = dt * P0.inv_inertia * A.w[k];  // w' = w + dt T / I
+    if (P0.coupleF) {
+        for (int k = 0; k < D; ++k) A.v[k] += dt * A.R[k];                                    // R' = R + dt v'
+        for (int k = 0; k < D; ++k) a.lamF[k] = dt * P0.inv_mass * A.v[k];                   // v' = v + dt F / m
+    }
+    // the field adjoint of tick n on the device
+    a.src = h->pop[h->cur];
+    a.lam_in = R.lam[R.lcur];
+    a.lam_out = R.lam[1 - R.lcur];
+    a.g = h->g;
+    for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
+    a.part = h->d_parts;
+    a.ivl = h->d_ivl;
+    a.has_part = 1;
+    a.rho0 = h->rho0;
+    a.inv_scale = 1.0 / h->scale;
+    a.dt = h->dt;
+    a.tau_p = h->tau;
+    a.tau_m = h->trt ? h->tau_minus : h->tau;
+    for (int k = 0; k < 3; ++k) a.F[k] = h->F[k];
+    a.guo = h->force_mode == LBM_FORCE_UNIFORM ? 1 : 0;
+    a.incompressible = h->incompressible;
+    a.rho_inc = h->rho_inc;
+    a.coeff = std::pow(h->dx, h->dims) / h->dt;
+    a.partial = R.partial;
+    h->ops.adjoint(a, h->stream);
+    k_adjoint_sum<kAdjAcc><<<1, 32, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
+    double acc[kAdjAcc];
+    CUDA_TRY(h, cudaMemcpyAsync(acc, R.dsum, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    R.lcur = 1 - R.lcur;
+    R.dtp += acc[0];
+    R.dtm += acc[1];
+    for (int k = 0; k < 3; ++k) R.dF[k] += acc[2 + k];
+    for (int k = 0; k < 12; ++k) A.S[k] += acc[5 + k];  // the snapshot tick n used
+    R.dB1 += acc[17];
+    R.dB2 += acc[18];
+    for (int k = 0; k < 3; ++k) A.mR[k] += acc[19 + k];
+    return LBM_OK;
+}
+
+// binomial coefficient C(s + r, s), saturating
+long long beta_sr(long long s, long long r) {
+    double b = 1.0;
+    for (long long k = 1; k <= r; ++k) {
+        b = b * (double)(s + k) / (double)k;
+        if (b > 4e18) return (long long)4e18;
+    }
+    return (long long)(b + 0.5);
+}
+
+// Reverse ticks [a, b) with the state at tick a on the device (and on top of
+// the snapshot stack) and `free` further snapshot slots.  Binomial
+// checkpointing: with r the fewest repetitions for which C(free + r, free)
+// covers the segment, the next checkpoint goes where the right part can
+// still be reversed with one slot fewer.
+int reverse(AdjointRun& R, long long a, long long b, int free) {
+    int rc;
+    if (b - a == 1) {
+        if (!R.have[b]) {  // the particle after the last tick: one tick ahead and back
+            if (free > 0) {
+                rc = snap_push(R);
+                if (!rc) rc = advance(R, 1);
+                if (!rc) rc = snap_restore(R, R.snaps.back());
+                if (rc) return rc;
+                snap_pop(R);
+            } else {
+                const Snap base = R.snaps.back();
+                rc = advance(R, 1);
+                if (!rc) rc = snap_restore(R, base);
+                if (!rc) rc = advance(R, a - base.tick);
+                if (rc) return rc;
+            }
+        }
+        return backward_tick(R, a);
+    }
+    if (free == 0) {  // no slot left: recompute from a for every tick
+        const Snap base = R.snaps.back();
+        for (long long t = b - 1; t >= a; --t) {
+            rc = LBM_OK;
+            if (!R.have[t + 1]) {
+                rc = snap_restore(R, base);
+                if (!rc) rc = advance(R, t + 1 - a);
+            }
+            if (!rc) rc = snap_restore(R, base);
+            if (!rc) rc = advance(R, t - a);
+            if (!rc) rc = backward_tick(R, t);
+            if (rc) return rc;
+        }
+        return LBM_OK;
+    }
+    const long long n = b - a;
+    long long r = 0;
+    while (beta_sr(free, r) < n) ++r;
+    const long long m = std::max<long long>(1, std::min<long long>(n - 1, n - beta_sr(free - 1, r)));
+    rc = advance(R, m);
+    if (!rc) rc = snap_push(R);
+    if (!rc) rc = reverse(R, a + m, b, free - 1);
+    if (rc) return rc;
+    snap_pop(R);
+    rc = snap_restore(R, R.snaps.back());
+    if (!rc) rc = reverse(R, a, a + m, free);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result* out) {
+    if (!h || !spec || !out) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (h->hparts.size() != 1) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint supports models with one particle");
+    if (h->has_walls) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support walls");
+    if (h->force_mode == LBM_FORCE_FIELD) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support force fields");
+    if (spec->ticks < 1 || spec->window_begin < 1 || spec->window_end < spec->window_begin ||
+        spec->window_end > spec->ticks)
+        return set_err(h, LBM_ERR_INVALID, "need 1 <= window_begin <= window_end <= ticks");
+    if (spec->snapshots < 2) return set_err(h, LBM_ERR_INVALID, "at least two snapshots");
+    if (h->tick != 0) return set_err(h, LBM_ERR_STATE, "the adjoint runs from tick 0 (a freshly built model)");
+    AdjointRun R;
+    R.h = h;
+    R.spec = *spec;
+    const long long T = spec->ticks;
+    R.rec.resize(T + 1);
+    R.have.assign(T + 1, 0);
+    R.have[0] = 1;
+    join_particles(h);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMemcpy(&R.rec[0], h->d_parts, sizeof(ParticleDev), cudaMemcpyDeviceToHost));
+    double en = 0.0;
+    for (int k = 0; k < 3; ++k) en += spec->direction[k] * spec->direction[k];
+    for (int k = 0; k < 3; ++k) R.e0[k] = en > 0 ? spec->direction[k] : R.rec[0].e[k];
+    for (auto& r : snap_regions(h)) R.snap_bytes += r.second;
+    const size_t lam_bytes = sizeof(double) * (size_t)h->N * h->q;
+    R.nblocks = (h->N + kAdjBlock - 1) / kAdjBlock;
+    int rc = dev_alloc(h, &R.lam[0], lam_bytes);
+    if (!rc) rc = dev_alloc(h, &R.lam[1], lam_bytes);
+    if (!rc) rc = dev_alloc(h, &R.partial, sizeof(double) * kAdjAcc * R.nblocks);
+    if (!rc) rc = dev_alloc(h, &R.dsum, sizeof(double) * kAdjAcc);
+    if (!rc && cudaMemset(R.lam[0], 0, lam_bytes) != cudaSuccess) rc = set_err(h, LBM_ERR_CUDA, "memset failed");
+    if (!rc) rc = snap_push(R);  // the initial state
+    if (!rc) rc = reverse(R, 0, T, spec->snapshots - 1);
+    if (!rc) {  // the initial condition depends on the body force
+        rc = snap_restore(R, R.snaps.front());
+        if (!rc && h->force_mode == LBM_FORCE_UNIFORM) {
+            AdjArgs a{};
+            a.src = h->pop[h->cur];
+            a.lam_in = R.lam[R.lcur];
+            a.g = h->g;
+            a.rho0 = h->rho0;
+            a.inv_scale = 1.0 / h->scale;
+            a.dt = h->dt;
+            a.guo = 1;
+            a.incompressible = h->incompressible;
+            a.rho_inc = h->rho_inc;
+            a.partial = R.partial;
+            h->ops.adjoint_init(a, h->stream);
+            k_adjoint_sum<kAdjAcc><<<1, 32, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
+            double acc[kAdjAcc];
+            // on the handle's stream: a plain cudaMemcpy would not wait for it
+            if (cudaMemcpyAsync(acc, R.dsum, sizeof(acc), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+                cudaStreamSynchronize(h->stream) != cudaSuccess)
+                rc = set_err(h, LBM_ERR_CUDA, "read-back failed");
+            else
+                for (int k = 0; k < 3; ++k) R.dF[k] += acc[k];
+        }
+    }
+    while (!R.snaps.empty()) snap_pop(R);
+    dev_free(R.lam[0]);
+    dev_free(R.lam[1]);
+    dev_free(R.partial);
+    dev_free(R.dsum);
+    h->device_bytes -= 2 * lam_bytes + sizeof(double) * kAdjAcc * (R.nblocks + 1);
+    if (rc) return rc;
+    std::memset(out, 0, sizeof(*out));
+    const double K = (double)(spec->window_end - spec->window_begin + 1);
+    double J = 0.0;
+    for (long long t = spec->window_begin; t <= spec->window_end; ++t)
+        for (int k = 0; k < h->dims; ++k) J += R.rec[t].v[k] * R.e0[k] / K;
+    out->value = J;
+    out->dB1 = R.dB1;
+    out->dB2 = R.dB2;
+    out->dtau_plus = R.dtp;
+    out->dtau_minus = h->trt ? R.dtm : 0.0;
+    out->dtau = R.dtp + (h->trt ? spec->tau_minus_slope * R.dtm : 0.0);
+    for (int k = 0; k < 3; ++k) out->dF[k] = k < h->dims ? R.dF[k] : 0.0;
+    out->forward_ticks = R.forward;
+    out->snapshots_used = R.max_used;
+    out->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return LBM_OK;
+}
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 #include "particles.cuh"
 #include "aux_kernels.cuh"
 #include "tick.cuh"
+#include "adjoint.cuh"
 
 namespace lbm {
 
@@ -26,6 +27,9 @@ struct Ops {
                  int* err, unsigned grid, cudaStream_t);
     // a batch's bulk tiles, one CTA per entry of dmap
     void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t);
+    // discrete adjoint of one tick, and of the initial condition (adjoint.cuh)
+    void (*adjoint)(const AdjArgs&, cudaStream_t);
+    void (*adjoint_init)(const AdjArgs&, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
     const void* fixup_fn;
     const void* tick_fn;
@@ -62,6 +66,12 @@ struct OpsImpl {
     static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s) {
         if constexpr (ST != ST_F64) k_bulk_batch<L, ST, TRT><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
     }
+    static void adjoint(const AdjArgs& a, cudaStream_t s) {
+        k_adjoint<L, ST, TRT><<<blocks_for(a.g.N, kAdjBlock), kAdjBlock, 0, s>>>(a);
+    }
+    static void adjoint_init(const AdjArgs& a, cudaStream_t s) {
+        k_adjoint_init<L, ST><<<blocks_for(a.g.N, kAdjBlock), kAdjBlock, 0, s>>>(a);
+    }
     static void encode(const CodecArgs& a, cudaStream_t s) { k_encode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void macro(const CodecArgs& a, cudaStream_t s) { k_macro<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
@@ -84,6 +94,8 @@ struct OpsImpl {
         o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
         o.tick = ST == ST_F64 ? nullptr : tick;
         o.bulk_batch = ST == ST_F64 ? nullptr : bulk_batch;
+        o.adjoint = adjoint;
+        o.adjoint_init = adjoint_init;
         o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
         o.fixup_fn = (const void*)k_fixup<L, ST, TRT>;
         o.tick_fn = nullptr;

@@ -103,32 +103,6 @@ __device__ __forceinline__ void tile_bits_update(const ParticleArgs& a, const in
     }
 }
 
-// exclusive prefix sum of one flag per thread over the CTA (at most 256 threads)
-__device__ __forceinline__ int block_scan(int flag, int* s_warp, int* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int v = flag;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int n = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += n;
-    }
-    if (lane == 31) s_warp[warp] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            const int t = s_warp[w];
-            s_warp[w] = run;
-            run += t;
-        }
-        s_warp[8] = run;
-    }
-    __syncthreads();
-    const int excl = s_warp[warp] + v - flag;
-    *total = s_warp[8];
-    __syncthreads();
-    return excl;
-}
-
 template <class L>
 __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int p) {
     constexpr int D = L::D;
@@ -137,7 +111,6 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty, s_keep;
     __shared__ unsigned long long s_slack;  // bit pattern of a non-negative double
     __shared__ unsigned s_links;
-    __shared__ int s_warp[9];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
     // the particle record is staged in shared memory: the update below is a
     // serial chain of reads and writes that must not go to global memory

@@ -139,6 +139,34 @@ class LbmBatchTuning(C.Structure):
     ]
 
 
+class LbmAdjointSpec(C.Structure):
+    _fields_ = [
+        ("ticks", C.c_int64),
+        ("window_begin", C.c_int64),
+        ("window_end", C.c_int64),
+        ("direction", C.c_double * 3),
+        ("tau_minus_slope", C.c_double),
+        ("snapshots", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class LbmAdjointResult(C.Structure):
+    _fields_ = [
+        ("value", C.c_double),
+        ("dB1", C.c_double),
+        ("dB2", C.c_double),
+        ("dtau", C.c_double),
+        ("dtau_plus", C.c_double),
+        ("dtau_minus", C.c_double),
+        ("dF", C.c_double * 3),
+        ("forward_ticks", C.c_int64),
+        ("snapshots_used", C.c_int32),
+        ("reserved", C.c_int32),
+        ("ms", C.c_double),
+    ]
+
+
 # (name, restype, argtypes) for every symbol of include/lbm_b200.h
 PROTOTYPES = [
     ("lbm_abi_version", C.c_int32, []),
@@ -164,6 +192,7 @@ PROTOTYPES = [
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_last_global_error", C.c_char_p, []),
     ("lbm_destroy", None, [C.c_void_p]),
+    ("lbm_adjoint", C.c_int, [C.c_void_p, C.POINTER(LbmAdjointSpec), C.POINTER(LbmAdjointResult)]),
     ("lbm_batch_create", C.c_int, [C.c_int32, C.POINTER(LbmConfig), C.POINTER(C.c_int32),
                                    C.POINTER(LbmParticleParams), C.POINTER(C.c_void_p)]),
     ("lbm_batch_size", C.c_int32, [C.c_void_p]),
