@@ -266,7 +266,7 @@ def run_ours(args):
                 "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
                 "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
-                "kernel": f"k_bulk_v4<D3Q19,{storage},TRT>", "bytes_per_launch": bulk_bytes,
+                "kernel": f"k_bulk_v4<D3Q19,{storage},TRT,64>", "bytes_per_launch": bulk_bytes,
                 "algorithmic_bytes_per_cell": 2 * q * bpp, "kernel_ms": kern,
                 "fixup_entries": prof.fixup_entries,
                 "timing": "value: CUDA events around the timed lbm_step call (graph replays); kernel_ms: mean of "
@@ -310,6 +310,7 @@ def run_ours(args):
                "sample": f"{ticks} ticks (after 1 warm-up tick) of the full {side}^3 workload, FP64 C++ restatement "
                          f"of the reference's GPU-module tick, OpenMP over cells ({dt:.1f} s)"}
     clocks = clk.summary()
+    forms = run_forms(args, local) if rank == 0 and world == 1 else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
@@ -322,12 +323,278 @@ def run_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                        "samples": clocks["samples"]},
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     m.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------
+# The three forms beside the plain FP32 path: shifted FP16/BF16 storage,
+# batches of replicas, and adjoint gradients.  Each entry states its config
+# and what its numbers were measured against.
+# ---------------------------------------------------------------------------
+def _ms_per_tick(m, n):
+    from lbmengine import _capi
+    lib = m._lib
+    lib.lbm_set_profiling(m.handle, 1)
+    m.step(n)
+    p = _capi.LbmProfile()
+    m._check(lib.lbm_get_profile(m.handle, p))
+    lib.lbm_set_profiling(m.handle, 0)
+    return p.total_ms / n
+
+
+def _rel_l2(a, b):
+    import numpy as np
+    return float(np.sqrt(np.sum((np.asarray(a) - np.asarray(b)) ** 2) / max(np.sum(np.asarray(b) ** 2), 1e-300)))
+
+
+def form_precision_c2(device):
+    """C2 workload per storage format: MLUPS over 5000 ticks (squirmer inside the
+    box throughout), and the error after 500 ticks against FP64 storage."""
+    from lbmengine import config, model as M
+    out = {"config": workload_name(128, "<storage>") + "; throughput over ticks 200..5200, error after 500 ticks",
+           "reference_for_error": "FP64 storage on the GPU (equal to the FP64 CPU oracle to 1e-10 in the parity tests)"}
+    fields = {}
+    for st in ("f32", "f16", "bf16", "f64"):
+        mkw, skw = workload(128, st, device=device)
+        m = M.LBMmodel(config.resolve_model(**mkw))
+        M._add(m, config.resolve_squirmer(3, **skw))
+        m.step(500)
+        fields[st] = (m.massDensity, m.fluidVelocity, list(m.particle_states()[0].position[:3]))
+        if st != "f64":
+            ms = _ms_per_tick(m, 5000)
+            out[st] = {"mlups": round(128 ** 3 / ms / 1e3, 1), "ms_per_tick": round(ms, 5)}
+        m.close()
+    import numpy as np
+    for st in ("f32", "f16", "bf16"):
+        rho, u, R = fields[st]
+        out[st].update(u_rel_l2=_rel_l2(u, fields["f64"][1]), rho_rel_l2=_rel_l2(rho, fields["f64"][0]),
+                       position_abs_err=float(np.max(np.abs(np.array(R) - np.array(fields["f64"][2])))))
+    for st in ("f16", "bf16"):
+        out[f"{st}_vs_f32"] = round(out[st]["mlups"] / out["f32"]["mlups"], 3)
+    return out
+
+
+def c3_particles(seed=3):
+    """64 non-overlapping squirmers of radius 6 in a 192^3 box: centres uniform in
+    [r+1, 190-r]^3 (0-based nodes) by rejection with centre distance >= 2r+2."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    r, side, centres = 6, 192, []
+    while len(centres) < 64:
+        c = rng.uniform(r + 1, side - 2 - r, 3)
+        if all(np.linalg.norm(c - q) >= 2 * r + 2 for q in centres):
+            centres.append(c)
+    parts = []
+    for c in centres:
+        e = rng.standard_normal(3)
+        parts.append(dict(radius=float(r), position=list(c - side // 2), swimmingSpeed=5e-4 / 1.5,
+                          beta=float(rng.uniform(-5, 5)), swimmingDirection=list(e / np.linalg.norm(e)),
+                          coupleForces=True, coupleTorques=True))
+    return parts
+
+
+def form_precision_c3(device, ticks=10000):
+    """C3: 192^3 D3Q19 TRT (tau 0.6, magic 1/4), 64 squirmers; FP16 and BF16
+    shifted storage against FP64 storage after `ticks` ticks."""
+    import numpy as np
+    from lbmengine import config, model as M
+    model = dict(dims=3, velocities="D3Q19", collisionModel="trt", kineticParameter=0.25, latticeParameter=1.0,
+                 relaxationTimeRatio=0.6, xlims=(-96.0, 95.0), device=device)
+    parts = c3_particles()
+    res = {}
+    out = {"config": f"D3Q19 TRT 192^3 periodic, tau=0.6, magic parameter 1/4, 64 squirmers r=6 (seeded, gap >= 2), "
+                     f"B1=5e-4, beta~U[-5,5]; {ticks} ticks; error against FP64 storage on the GPU"}
+    for st in ("f64", "f16", "bf16", "f32"):
+        m = M.LBMmodel(config.resolve_model(**dict(model, storage=st)))
+        for p in parts:
+            M._add(m, config.resolve_squirmer(3, **p))
+        ms = _ms_per_tick(m, ticks)
+        R = np.array([ps.position[:3] for ps in m.particle_states()])
+        res[st] = (m.massDensity, m.fluidVelocity, R)
+        out[st] = {"mlups": round(192 ** 3 / ms / 1e3, 1), "ms_per_tick": round(ms, 5)}
+        m.close()
+    for st in ("f16", "bf16", "f32"):
+        rho, u, R = res[st]
+        d = np.linalg.norm(R - res["f64"][2], axis=1)
+        out[st].update(u_rel_l2=_rel_l2(u, res["f64"][1]), rho_rel_l2=_rel_l2(rho, res["f64"][0]),
+                       position_err_max=float(d.max()), position_err_mean=float(d.mean()))
+    return out
+
+
+def c4_replicas(n=512, seed=4):
+    """C4: D2Q9 TRT squirmer replicas: side in {64,96,128,192,256}, radius in
+    6..12, beta~U[-5,5], tau~U[0.55,1], B1=1e-3, seeded centre and orientation."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n):
+        side = int(rng.choice([64, 96, 128, 192, 256]))
+        r = int(rng.integers(6, 13))
+        beta, tau, ang = float(rng.uniform(-5, 5)), float(rng.uniform(0.55, 1.0)), float(rng.uniform(0, 2 * np.pi))
+        h = side // 2
+        pos = [float(rng.uniform(r + 1, side - 2 - r)) - h for _ in range(2)]
+        specs.append((dict(dims=2, latticeParameter=1.0, relaxationTimeRatio=tau, collisionModel="trt",
+                           xlims=(-float(h), float(side - h - 1))),
+                      [("squirmer", dict(radius=float(r), position=pos, swimmingSpeed=1e-3 / 1.5, beta=beta,
+                                         swimmingDirection=[float(np.cos(ang)), float(np.sin(ang))],
+                                         coupleForces=True, coupleTorques=True))]))
+    return specs
+
+
+def form_batch(device, ticks=2000, sampled=8):
+    import numpy as np
+    from lbmengine import LBMbatch, config, model as M
+    specs = c4_replicas()
+    for mkw, _ in specs:
+        mkw["device"] = device
+    b = LBMbatch(specs)
+    chosen, cands = b.autotune(ticks=32)
+    b.set_profiling(1)
+    b.step(ticks)
+    ms = b.profile().total_ms / ticks
+    out = {"config": f"512 D2Q9 TRT squirmer replicas (side in {{64..256}}, r 6..12, beta~U[-5,5], tau~U[0.55,1], "
+                     f"B1=1e-3), {ticks} ticks, FP32", "cells": b.cells,
+           "mlups": round(b.cells / ms / 1e3, 1), "ms_per_tick": round(ms, 5),
+           "tuning": vars(chosen), "candidates": len(cands),
+           "hbm_frac_of_measured": round(b.cells * 72 / (ms / 1e3) / 1e9 / measured_peak()[0], 4)}
+    # the same replicas one at a time (each model's own graph-replayed tick)
+    tot = 0.0
+    for mkw, parts in specs:
+        m = M.LBMmodel(config.resolve_model(**mkw))
+        for _, pkw in parts:
+            M._add(m, config.resolve_squirmer(2, **pkw))
+        m.step(16)
+        tot += _ms_per_tick(m, 32)
+        m.close()
+    out["one_at_a_time_mlups"] = round(b.cells / tot / 1e3, 1)
+    out["batch_vs_one_at_a_time"] = round(tot / ms, 2)
+    # per-replica error against the FP64 CPU oracle on sampled replicas
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the checker
+    oracle.build()
+    idx = sorted(np.random.default_rng(8).choice(len(specs), sampled, replace=False).tolist())
+    errs = []
+    for i in idx:
+        mkw, parts = specs[i]
+        orc = oracle.OracleModel(config.resolve_model(**mkw))
+        orc.add_particle(config.resolve_squirmer(2, **parts[0][1]))
+        orc.step(ticks)
+        rho_o, u_o = orc.fields()
+        rep = b.replicas[i]
+        R_o = np.array(orc.particles()[0].position[:2])
+        errs.append({"replica": i, "side": rep._shape[0],
+                     "u_rel_l2": _rel_l2(rep.fluidVelocity.reshape(-1, 2, order="F").T, u_o),
+                     "rho_rel_l2": _rel_l2(rep.massDensity.ravel(order="F"), rho_o),
+                     "position_abs_err": float(np.max(np.abs(np.array(rep.particle_states()[0].position[:2]) - R_o)))})
+        orc.close()
+    out["oracle_check"] = errs
+    b.close()
+    return out
+
+
+def c5_case(side=96, storage="f32"):
+    h = side // 2
+    model = dict(dims=3, velocities="D3Q19", collisionModel="trt", kineticParameter=3 / 16, latticeParameter=1.0,
+                 relaxationTimeRatio=0.7, xlims=(-float(h), float(side - h - 1)), forceDensity=[1e-6, 0.0, 0.0],
+                 storage=storage)
+    squirmer = dict(radius=8.0, position=[0.0, 0.0, 0.0], swimmingSpeed=5e-4 / 1.5, beta=-2.0,
+                    swimmingDirection=unit_vector(2024, 3), coupleForces=True, coupleTorques=True)
+    return model, squirmer
+
+
+def form_gradients(device, ticks=3000, window=(1000, 3000), dual_side=32):
+    import numpy as np
+    from lbmengine.adjoint import build_swimmer, swimming_speed_gradient
+    out = {"config": f"D3Q19 TRT 96^3, one squirmer r=8, B1=5e-4, beta=-2, tau=0.7 (magic 3/16), F=(1e-6,0,0); "
+                     f"observable: velocity along the initial orientation averaged over ticks {window[0]}..{window[1]}; "
+                     f"at most 32 stored states"}
+    for st in ("f32", "f64"):
+        mkw, skw = c5_case(96, st)
+        mkw["device"] = device
+        m = build_swimmer(mkw, skw)
+        g = swimming_speed_gradient(m, ticks, window, snapshots=32)
+        m.close()
+        out[st] = {"value": g.value, "grad": g.grad, "ms": round(g.ms, 1), "forward_ticks": g.forward_ticks,
+                   "snapshots_used": g.snapshots_used}
+    # central differences of FP64 forward runs
+    mkw, skw = c5_case(96, "f64")
+    mkw["device"] = device
+    B1 = 1.5 * skw["swimmingSpeed"]
+    theta = np.array([B1, skw["beta"] * B1, 0.7, 1e-6, 0.0, 0.0])
+
+    def observable(th):
+        m = build_swimmer(mkw, skw, th)
+        e0 = np.array(skw["swimmingDirection"])
+        J = 0.0
+        for t in range(1, ticks + 1):
+            m.step(1)
+            if window[0] <= t <= window[1]:
+                J += float(np.dot(m.particle_states()[0].velocity[:3], e0)) / (window[1] - window[0] + 1)
+        m.close()
+        return J
+
+    fd = {}
+    for rel in (1e-4, 1e-6):
+        fd[str(rel)] = {}
+        for k, nm in enumerate(("B1", "B2", "tau", "Fx")):
+            h = rel * abs(theta[k])
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            d = (observable(tp) - observable(tm)) / (2 * h)
+            fd[str(rel)][nm] = {"fd": d, "rel_err_f64_adjoint": abs(out["f64"]["grad"][nm] - d) / abs(d),
+                                "rel_err_f32_adjoint": abs(out["f32"]["grad"][nm] - d) / abs(d)}
+    out["central_differences"] = fd
+    # forward-mode dual numbers through the CPU oracle on the same setup at dual_side^3
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the checker
+    from lbmengine import config
+    oracle.build()
+    mkw, skw = c5_case(dual_side, "f64")
+    res = config.resolve_model(**mkw)
+    t0 = time.perf_counter()
+    dual = oracle.DualOracle(res)
+    p = config.resolve_squirmer(3, **skw)
+    dual.add_particle(p)
+    e0 = np.array(p.swimming_direction[:3])
+    dJ = np.zeros(len(oracle.DIRECTIONS))
+    for t in range(1, ticks + 1):
+        dual.step(1)
+        if window[0] <= t <= window[1]:
+            _, der = dual.particle(1)
+            dJ += (e0 @ der["velocity"][:3]) / (window[1] - window[0] + 1)
+    dual.close()
+    dual_s = time.perf_counter() - t0
+    m = build_swimmer(dict(mkw, device=device), skw)
+    g = swimming_speed_gradient(m, ticks, window, snapshots=32)
+    m.close()
+    out["dual_check"] = {"side": dual_side, "cpu_seconds": round(dual_s, 1),
+                         "rel_err": {nm: abs(g.grad[nm] - v) / abs(v) for nm, v in zip(oracle.DIRECTIONS, dJ)
+                                     if abs(v) > 0}}
+    return out
+
+
+def run_forms(args, device):
+    forms = {}
+    for name, fn in (("precision_c2", lambda: form_precision_c2(device)),
+                     ("precision_c3", lambda: form_precision_c3(device)),
+                     ("batching_c4", lambda: form_batch(device)),
+                     ("gradients_c5", lambda: form_gradients(device))):
+        if name in args.skip_forms:
+            continue
+        t0 = time.perf_counter()
+        try:
+            forms[name] = fn()
+        except Exception as exc:  # reported, not hidden: the form's entry carries the error
+            forms[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        forms[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+    return forms
 
 
 def main(argv=None):
@@ -341,7 +608,12 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--cpu-ticks", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-forms", default="",
+                    help="comma-separated forms to skip: precision_c2, precision_c3, batching_c4, gradients_c5 "
+                         "(all: skip every form)")
     args = ap.parse_args(argv)
+    args.skip_forms = {"precision_c2", "precision_c3", "batching_c4", "gradients_c5"} \
+        if args.skip_forms == "all" else set(filter(None, args.skip_forms.split(",")))
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
