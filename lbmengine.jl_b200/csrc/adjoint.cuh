@@ -162,6 +162,78 @@ __device__ __forceinline__ void slip_velocity_t(const T* sR, const T* sV, const 
     for (int k = 0; k < 3; ++k) out[k] = first * (edr * ur[k] - (k < D ? sE[k] : lift<T>(0.0))) + bulk[k];
 }
 
+// The transposed derivatives of the collision at fixed f, contracted with
+// lam*: with feq_i(rho, u), the Guo term G_i(u, F, tau+-) and
+//   TRT  f*_i = f_i - w+ (f+_i - feq+_i) - w- (f-_i - feq-_i) + G_i,  w+- = dt / tau+-
+//   BGK  f*_i = f_i - w (f_i - feq_i) + G_i
+// sum_i lam*_i d f*_i / d theta = sum_i mu_i d feq_i / d theta + sum_i lam*_i d G_i / d theta
+// (+ the tau terms of w+-), where mu_i = w+ (lam*_i + lam*_opp)/2 + w- (lam*_i - lam*_opp)/2.
+// Outputs: d/drho, d/du_k, d/dtau+, d/dtau-, d/dF_k (u held fixed).
+template <class L, bool TRT>
+__device__ __forceinline__ void collide_vjp(const double* f, const double* ls, double rho, const double* u,
+                                            const AdjArgs& a, double& g_rho, double* g_u, double& g_tp,
+                                            double& g_tm, double* g_F) {
+    constexpr int Q = L::Q, D = L::D;
+    const double dt = a.dt;
+    const double wp = dt / a.tau_p, wm = TRT ? dt / a.tau_m : wp;
+    const double ap = 1.0 - dt / (2.0 * a.tau_p), am = TRT ? 1.0 - dt / (2.0 * a.tau_m) : ap;
+    const double dap = dt / (2.0 * a.tau_p * a.tau_p), dam = TRT ? dt / (2.0 * a.tau_m * a.tau_m) : 0.0;
+    double uu = 0.0, uF = 0.0;
+    for (int k = 0; k < D; ++k) {
+        uu += u[k] * u[k];
+        uF += u[k] * a.F[k];
+    }
+    g_rho = 0.0;
+    g_tp = g_tm = 0.0;
+    for (int k = 0; k < 3; ++k) g_u[k] = g_F[k] = 0.0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int ib = L::opp(i);
+        const double c[3] = {(double)L::cx(i), (double)L::cy(i), (double)L::cz(i)};
+        const double w = L::w(i);
+        double uc = 0.0, cF = 0.0;
+        for (int k = 0; k < D; ++k) {
+            uc += u[k] * c[k];
+            cF += c[k] * a.F[k];
+        }
+        const double second = 3.0 * uc + 4.5 * uc * uc - 1.5 * uu;
+        const double scale = a.incompressible ? a.rho_inc : rho;  // the factor of the velocity terms
+        const double eq = a.incompressible ? w * rho + w * a.rho_inc * second : w * rho * (1.0 + second);
+        const double mu = TRT ? 0.5 * wp * (ls[i] + ls[ib]) + 0.5 * wm * (ls[i] - ls[ib]) : wp * ls[i];
+        g_rho += mu * (a.incompressible ? w : w * (1.0 + second));
+        for (int k = 0; k < D; ++k) g_u[k] += mu * w * scale * (3.0 * c[k] + 9.0 * uc * c[k] - 3.0 * u[k]);
+        // relaxation rates: d w+-/d tau+- = -dt / tau+-^2 times -(f+- - feq+-)
+        if (TRT) {
+            const double eqb = a.incompressible ? w * rho + w * a.rho_inc * (3.0 * (-uc) + 4.5 * uc * uc - 1.5 * uu)
+                                                : w * rho * (1.0 + (3.0 * (-uc) + 4.5 * uc * uc - 1.5 * uu));
+            const double fp = 0.5 * (f[i] + f[ib]) - 0.5 * (eq + eqb), fm = 0.5 * (f[i] - f[ib]) - 0.5 * (eq - eqb);
+            g_tp += ls[i] * (wp / a.tau_p) * fp;
+            g_tm += ls[i] * (wm / a.tau_m) * fm;
+        } else {
+            g_tp += ls[i] * (wp / a.tau_p) * (f[i] - eq);
+        }
+        if (a.guo) {
+            const double lw = ls[i] * w * dt;
+            if (TRT) {
+                // G = w dt [a+ (-3 u.F + 9 uc cF) + a- 3 cF]
+                for (int k = 0; k < D; ++k) {
+                    g_u[k] += lw * ap * (-3.0 * a.F[k] + 9.0 * c[k] * cF);
+                    g_F[k] += lw * (ap * (-3.0 * u[k] + 9.0 * uc * c[k]) + am * 3.0 * c[k]);
+                }
+                g_tp += lw * dap * (-3.0 * uF + 9.0 * uc * cF);
+                g_tm += lw * dam * 3.0 * cF;
+            } else {
+                // G = w dt a (3 (c - u).F + 9 uc cF)
+                for (int k = 0; k < D; ++k) {
+                    g_u[k] += lw * ap * (-3.0 * a.F[k] + 9.0 * c[k] * cF);
+                    g_F[k] += lw * ap * (3.0 * (c[k] - u[k]) + 9.0 * uc * c[k]);
+                }
+                g_tp += lw * dap * (3.0 * (cF - uF) + 9.0 * uc * cF);
+            }
+        }
+    }
+}
+
 template <class L, int ST, bool TRT>
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(const AdjArgs a) {
     using SS = Store<ST>;
@@ -271,31 +343,16 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(const AdjArgs a) {
                 }
             }
         }
-        // 3. transposed collision: derivatives of f* at fixed f along rho,
-        //    u_k, tau+, tau-, F_k, then the chain through rho(f), u(f)
+        // 3. transposed collision at fixed f, then the chain through rho(f), u(f)
         double mu_u[3] = {0, 0, 0};
-        for (int dir = 0; dir < 9; ++dir) {
-            if (!live && dir < 4) continue;
-            if (dir >= 1 && dir <= 3 && dir - 1 >= D) continue;
-            if (dir >= 6 && (dir - 6 >= D || !a.guo)) continue;
-            if (dir == 5 && !TRT) continue;
-            const DD1 r_ = dd(rho, dir == 0 ? 1.0 : 0.0);
-            DD1 u_[3], F_[3];
-            for (int k = 0; k < 3; ++k) {
-                u_[k] = dd(u[k], dir == 1 + k ? 1.0 : 0.0);
-                F_[k] = dd(a.F[k], dir == 6 + k ? 1.0 : 0.0);
-            }
-            DD1 o[L::Q];
-            ref_collide<L, TRT, DD1>(f, r_, u_, dd(a.tau_p, dir == 4 ? 1.0 : 0.0), dd(a.tau_m, dir == 5 ? 1.0 : 0.0),
-                                     F_, a, o);
-            double g = 0.0;
-#pragma unroll
-            for (int i = 0; i < Q; ++i) g += ls[i] * o[i].d;
-            if (dir == 0) mu_rho += g;
-            else if (dir <= 3) mu_u[dir - 1] = g;
-            else if (dir == 4) acc[0] += g;
-            else if (dir == 5) acc[1] += g;
-            else acc[2 + dir - 6] += g;
+        {
+            double g_rho, g_tp, g_tm, g_F[3];
+            collide_vjp<L, TRT>(f, ls, rho, u, a, g_rho, mu_u, g_tp, g_tm, g_F);
+            if (live) mu_rho += g_rho;
+            else mu_u[0] = mu_u[1] = mu_u[2] = 0.0;
+            acc[0] += g_tp;
+            acc[1] += TRT ? g_tm : 0.0;
+            for (int k = 0; k < D; ++k) acc[2 + k] += g_F[k];
         }
         if (live && a.guo)
             for (int k = 0; k < D; ++k) acc[2 + k] += mu_u[k] * 0.5 * a.dt / rho;  // u = (J + dt F / 2) / rho
@@ -375,14 +432,24 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint_init(const AdjArgs a) {
     }
 }
 
-// sum of the per-CTA accumulators in CTA order (deterministic)
+// Sum of the per-CTA accumulators, one CTA per accumulator: thread t adds
+// the CTAs t, t + 256, ... in order, then a fixed tree over the threads, so
+// the result does not depend on scheduling.
+constexpr int kSumBlock = 256;
 template <int NA>
-__global__ void k_adjoint_sum(const double* __restrict__ partial, long long nblocks, double* out) {
-    const int k = threadIdx.x;
-    if (k >= NA) return;
+__global__ void __launch_bounds__(kSumBlock) k_adjoint_sum(const double* __restrict__ partial, long long nblocks,
+                                                          double* out) {
+    __shared__ double s[kSumBlock];
+    const int k = blockIdx.x;
     double v = 0.0;
-    for (long long b = 0; b < nblocks; ++b) v += partial[b * NA + k];
-    out[k] = v;
+    for (long long b = threadIdx.x; b < nblocks; b += kSumBlock) v += partial[b * NA + k];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = kSumBlock / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = s[0];
 }
 
 }  // namespace lbm

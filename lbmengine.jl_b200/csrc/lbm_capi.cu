@@ -2395,7 +2395,7 @@ int backward_tick(AdjointRun& R, long long n) {
     a.coeff = std::pow(h->dx, h->dims) / h->dt;
     a.partial = R.partial;
     h->ops.adjoint(a, h->stream);
-    k_adjoint_sum<kAdjAcc><<<1, 32, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
+    k_adjoint_sum<kAdjAcc><<<kAdjAcc, kSumBlock, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
     double acc[kAdjAcc];
     CUDA_TRY(h, cudaMemcpyAsync(acc, R.dsum, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -2528,7 +2528,7 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
             a.rho_inc = h->rho_inc;
             a.partial = R.partial;
             h->ops.adjoint_init(a, h->stream);
-            k_adjoint_sum<kAdjAcc><<<1, 32, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
+            k_adjoint_sum<kAdjAcc><<<kAdjAcc, kSumBlock, 0, h->stream>>>(R.partial, R.nblocks, R.dsum);
             double acc[kAdjAcc];
             // on the handle's stream: a plain cudaMemcpy would not wait for it
             if (cudaMemcpyAsync(acc, R.dsum, sizeof(acc), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
