@@ -228,7 +228,7 @@ typedef struct lbm_profile {
     int64_t launches;       /* kernel launches enqueued by the call */
     int64_t profiled_steps; /* ticks whose kernels were bracketed by events */
     int64_t bulk_cells;     /* lattice nodes updated by the bulk kernel per tick */
-    int64_t fixup_entries;  /* nodes the boundary fix-up examines per tick (particle near boxes + wall-link nodes) */
+    int64_t fixup_entries;  /* nodes the boundary fix-up visits per tick (particle link nodes + wall-link nodes) */
 } lbm_profile;
 
 /* level 0: off; 1: device time of each lbm_step call; 2: also per-kernel

@@ -1,12 +1,13 @@
 // Fix-up kernel: boundary links and walls.
 //
 // CTA kinds (blockIdx.x):
-//   [0, nparts*maxchunks)            chunk `c` (kFixBlock nodes) of particle p's near box;
+//   [0, nparts*maxchunks)            chunk `c` (kFixBlock entries) of particle p's link list;
 //   [.., + ceil(nwlinks/kFixBlock))  static wall-link entries (cell, direction mask);
 //   [.., + ceil(nwnodes/kFixBlock))  wall nodes (reset to f = 0).
-// A particle CTA derives each node's link mask from the particle's solid row
-// intervals: bit j is set when the node is fluid for the particle and its
-// source x - c_j is solid (streamingInvasionRegions, src/gpu/aux.jl:187-198).
+// A particle's link list (built by the particle update whenever its solid
+// intervals change) holds the fluid nodes x of its near box with mask bit j
+// set where x - c_j is solid (streamingInvasionRegions, src/gpu/aux.jl:187-198);
+// chunks past the list's length return at once.
 // The value written to slot (x, j) follows tick! (fluids.jl:143-206) for the
 // whole region (walls and every particle):
 //     f*_opp(j)(x)  (+ moving wall term)  (+ Ladd terms of the particles, in
@@ -23,7 +24,6 @@
 
 namespace lbm {
 
-constexpr int kFixIvl = 512;    // particle interval rows staged in shared memory
 constexpr int kFixCoord = 64;   // near-box node coordinates staged per axis
 
 template <class L, int ST, bool TRT>
@@ -39,7 +39,6 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
     __shared__ R s_g[Q][kFixBlock];
     __shared__ double s_red[kFixBlock / 32][6];
     __shared__ ParticleDev sP;
-    __shared__ int2 s_ivl[kFixIvl];
     __shared__ double s_X[3][kFixCoord];
     __shared__ int s_alone;
     const int tid = threadIdx.x;
@@ -63,7 +62,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
     if (is_part) {
         p = (int)(b / a.maxchunks);
         chunk = (int)(b % a.maxchunks);
-        if (chunk * kFixBlock >= near_volume(a.parts[p], a.g, D)) return;  // uniform: chunk outside the near box
+        if (chunk * kFixBlock >= a.parts[p].nlinks) return;  // uniform: chunk past the link list
         const unsigned long long* gsrc = reinterpret_cast<const unsigned long long*>(a.parts + p);
         unsigned long long* sdst = reinterpret_cast<unsigned long long*>(&sP);
         for (int k = tid; k < (int)(sizeof(ParticleDev) / 8); k += kFixBlock) sdst[k] = gsrc[k];
@@ -104,57 +103,36 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         }
     }
     if (is_part && a.wall && tid == 0) s_alone = 0;
-    // the owner's solid intervals and near-box coordinates
-    int rows = 0, ly = 1;
+    // the owner's near-box coordinates, and this thread's entry of the link list
     int ext[3] = {1, 1, 1};
     if (is_part)
         for (int k = 0; k < D; ++k) ext[k] = near_extent(sP, a.g, k, D);
     const bool cst = is_part && ext[0] <= kFixCoord && ext[1] <= kFixCoord && ext[2] <= kFixCoord;
+    bool valid = false;
+    int cell = 0, x = 0, y = 0, z = 0;
+    unsigned mask = 0;
     if (is_part) {
-        ly = sP.shi[1] - sP.slo[1] + 1;
-        rows = ly * (sP.shi[2] - sP.slo[2] + 1);
-        if (rows <= kFixIvl)
-            for (int r = tid; r < rows; r += kFixBlock) s_ivl[r] = a.ivl[sP.ivl_off + r];
         if (cst)
             for (int k = 0; k < D; ++k)
                 for (int i = tid; i < ext[k]; i += kFixBlock)
                     s_X[k][i] = a.coord[k][wrap_idx(sP.slo[k] - 1 + i, a.g.n[k])];
+        const int e = chunk * kFixBlock + tid;
+        if (e < sP.nlinks) {
+            const int2 ent = a.links[sP.link_off + e];
+            cell = ent.x;
+            mask = (unsigned)ent.y;
+            x = cell % nx;
+            y = (cell / nx) % ny;
+            z = cell / (nx * ny);
+            valid = true;
+        }
     }
     __syncthreads();
     // coordinate of node index i on axis k (staged for the owner's near box)
     auto coordf = [&](int k, int i) -> double {
         return cst ? s_X[k][wrap_idx(i - (sP.slo[k] - 1), a.g.n[k])] : a.coord[k][i];
     };
-    auto owner_solid = [&](int qx, int qy, int qz) -> bool {
-        if (qy < sP.slo[1] || qy > sP.shi[1] || qz < sP.slo[2] || qz > sP.shi[2]) return false;
-        const int r = (qy - sP.slo[1]) + ly * (qz - sP.slo[2]);
-        const int2 iv = rows <= kFixIvl ? s_ivl[r] : a.ivl[sP.ivl_off + r];
-        return qx >= iv.x && qx <= iv.y;
-    };
-
-    // the node of this thread and its link mask
-    bool valid = false;
-    int cell = 0, x = 0, y = 0, z = 0;
-    unsigned mask = 0;
-    if (is_part) {
-        const int e0 = near_extent(sP, a.g, 0, D), e1 = near_extent(sP, a.g, 1, D);
-        const int v = chunk * kFixBlock + tid;
-        if (v < near_volume(sP, a.g, D)) {
-            x = wrap_idx(sP.slo[0] - 1 + v % e0, nx);
-            y = wrap_idx(sP.slo[1] - 1 + (v / e0) % e1, ny);
-            z = D == 3 ? wrap_idx(sP.slo[2] - 1 + v / (e0 * e1), nz) : 0;
-            if (!owner_solid(x, y, z)) {
-                for (int j = 1; j < Q; ++j) {
-                    const int i = s_lat[3][j];  // source x - c_j = x + c_i
-                    if (owner_solid(wrap_idx(x + s_lat[0][i], nx), wrap_idx(y + s_lat[1][i], ny),
-                                    wrap_idx(z + s_lat[2][i], nz)))
-                        mask |= 1u << j;
-                }
-            }
-            cell = x + nx * (y + ny * z);
-            valid = mask != 0;
-        }
-    } else {
+    if (!is_part) {
         const long long e = (b - npb) * kFixBlock + tid;
         if (e < a.nwlinks) {
             const int2 ent = a.wlinks[e];

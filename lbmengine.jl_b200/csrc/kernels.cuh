@@ -66,7 +66,8 @@ struct ParticleDev {
     int link_off, link_cap;  // boundary-link entries (cell, direction mask)
     int nlinks;              // entries in use
     int part_off;            // partial-sum slots: one per chunk of kFixBlock entries
-    int pad0, pad1;
+    int relink;              // the link list must be rebuilt (k_links, k_links_sort) before the next fix-up
+    int pad1;
 };
 
 struct StepArgs {

@@ -93,6 +93,9 @@ struct lbm_handle {
     double* d_partial = nullptr;
     long long partial_slots = 0;
     int maxchunks = 0;
+    int link_bpp = 1;  // link-rebuild CTAs per particle (largest near box / kLinkBlock)
+    int* d_linkcnt = nullptr;  // [particle capacity][link_bpp] per-CTA link counts
+    long long linkcnt_slots = 0;
     int* d_err = nullptr;
     double* d_tmp = nullptr;  // FP64 read-back / upload scratch
     size_t tmp_bytes = 0;
@@ -313,6 +316,7 @@ ParticleArgs particle_args(const lbm_handle* h, int mode, int pid, int src = -1)
     a.parts = h->d_parts;
     a.nparts = (int)h->hparts.size();
     a.mode = mode;
+    a.inline_links = mode != 0 ? 1 : 0;  // setup rebuilds its list at once
     a.setup_pid = pid;
     a.words = h->words;
     a.partial = h->d_partial;
@@ -385,6 +389,7 @@ int prepare_tick(lbm_handle* h) {
         ta[s] = step_args(h, s);
         ta[s].nbox = h->d_nbox[1 - s];  // boxes of the previous tick's update (see tick.cuh)
         pa[s] = particle_args(h, 0, 0, s);
+        pa[s].inline_links = 1;  // no separate link kernels inside the persistent tick
     }
     dev_free(h->d_amap);
     dev_free(h->d_bmap);
@@ -420,7 +425,7 @@ int prepare_tick(lbm_handle* h) {
 int launches_per_tick(const lbm_handle* h) {
     if (use_tick_kernel(h)) return 1;
     const bool fix = fixup_blocks(h) > 0;
-    return 1 + (fix ? 1 : 0) + (h->hparts.empty() ? 0 : 1);
+    return 1 + (fix ? 1 : 0) + (h->hparts.empty() ? 0 : 3);  // particles, links, links_sort
 }
 
 // events of graph slot s: [0] before bulk, [1] after bulk, [2] after fix-up, [3] after particles
@@ -464,7 +469,9 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
         cudaEventRecord(h->ev_fix, h->stream);
         cudaStreamWaitEvent(h->side, h->ev_fix, 0);
         prof_record(h, slot, 2, h->side);
-        h->ops.particles(particle_args(h, 0, 0, src), (unsigned)a.nparts, h->side);
+        const ParticleArgs pa = particle_args(h, 0, 0, src);
+        h->ops.particles(pa, (unsigned)a.nparts, h->side);
+        h->ops.links(pa, a.nparts, h->link_bpp, h->d_linkcnt, h->side);
         prof_record(h, slot, 3, h->side);
         cudaEventRecord(h->ev_part, h->side);
         h->part_pending = true;
@@ -572,6 +579,7 @@ void destroy_all(lbm_handle* h) {
     dev_free(h->d_parts);
     dev_free(h->d_ivl);
     dev_free(h->d_links);
+    dev_free(h->d_linkcnt);
     dev_free(h->d_partial);
     dev_free(h->d_err);
     dev_free(h->d_tmp);
@@ -1028,6 +1036,9 @@ int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_ou
     CUDA_TRY(h, cudaMemcpyAsync(h->d_parts + pid, &P, sizeof(P), cudaMemcpyHostToDevice, h->stream));
     h->hparts.push_back(P);
     h->maxchunks = std::max<int>(h->maxchunks, (int)chunks);
+    h->link_bpp = std::max<int>(h->link_bpp, (int)((near + kLinkBlock - 1) / kLinkBlock));
+    rc = grow(h, &h->d_linkcnt, &h->linkcnt_slots, (long long)(pid + 1) * h->link_bpp, 0);
+    if (rc) return rc;
     drop_graphs(h);
     // initial setup: moveParticles!(initialSetup = true)
     h->ops.particles(particle_args(h, 1, pid), 1, h->stream);
@@ -1100,7 +1111,7 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
         if (!h->hparts.empty()) {
             std::vector<ParticleDev> tmp(h->hparts.size());
             CUDA_TRY(h, cudaMemcpy(tmp.data(), h->d_parts, sizeof(ParticleDev) * tmp.size(), cudaMemcpyDeviceToHost));
-            for (const auto& q : tmp) entries += near_volume(q, h->g, h->dims);
+            for (const auto& q : tmp) entries += q.nlinks;
         }
         p.fixup_entries = entries;
     }
@@ -1171,7 +1182,9 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
             h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
             b = 1 - b;
         } else {
-            h->ops.particles(particle_args(h, 0, 0, b), (unsigned)np, h->stream);
+            const ParticleArgs pa = particle_args(h, 0, 0, b);
+            h->ops.particles(pa, (unsigned)np, h->stream);
+            h->ops.links(pa, np, h->link_bpp, h->d_linkcnt, h->stream);
         }
     }
     CUDA_TRY(h, cudaEventRecord(e1, h->stream));
@@ -1590,7 +1603,10 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
         pa.nbox_out[0] = h->d_nbox[h->cur];
         launch_bulk(h, a, h->stream);
         if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
-        if (np > 0) h->ops.particles(pa, (unsigned)np, h->stream);
+        if (np > 0) {
+            h->ops.particles(pa, (unsigned)np, h->stream);
+            h->ops.links(pa, np, h->link_bpp, h->d_linkcnt, h->stream);
+        }
         h->cur = 1 - h->cur;
     }
     CUDA_TRY(h, cudaGetLastError());
@@ -1731,6 +1747,7 @@ int batch_prepare(lbm_batch* b) {
             a.err = b->d_err + r;
             ParticleArgs& q = pa[(size_t)s * n + r];
             q = particle_args(h, 0, 0, src);
+            q.inline_links = 1;  // the queue has no separate link kernels
             q.err = b->d_err + r;
         }
     }

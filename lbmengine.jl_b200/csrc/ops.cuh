@@ -14,6 +14,9 @@ struct Ops {
     void (*bulk)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
     void (*fixup)(const StepArgs&, unsigned grid, cudaStream_t);
     void (*particles)(const ParticleArgs&, unsigned grid, cudaStream_t);
+    // link-list rebuild of flagged particles: two passes of blocks_per_particle
+    // CTAs per particle; counts holds nparts * blocks_per_particle ints
+    void (*links)(const ParticleArgs&, int nparts, int blocks_per_particle, int* counts, cudaStream_t);
     void (*encode)(const CodecArgs&, cudaStream_t);
     void (*decode)(const CodecArgs&, cudaStream_t);
     void (*macro)(const CodecArgs&, cudaStream_t);
@@ -50,6 +53,11 @@ struct OpsImpl {
     static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
         k_particles<L><<<grid, kPartBlock, 0, s>>>(a);
     }
+    static void links(const ParticleArgs& a, int nparts, int bpp, int* counts, cudaStream_t s) {
+        if (nparts <= 0) return;
+        k_links_count<L><<<(unsigned)(nparts * bpp), kLinkBlock, 0, s>>>(a, bpp, counts);
+        k_links_write<L><<<(unsigned)(nparts * bpp), kLinkBlock, 0, s>>>(a, bpp, counts);
+    }
     static void bulk_v4(const StepArgs& a, long long tiles, int block, cudaStream_t s) {
         if constexpr (ST != ST_F64) {
             const unsigned g = (unsigned)tiles;
@@ -85,6 +93,7 @@ struct OpsImpl {
         o.bulk = bulk;
         o.fixup = fixup;
         o.particles = particles;
+        o.links = links;
         o.encode = encode;
         o.decode = decode;
         o.macro = macro;

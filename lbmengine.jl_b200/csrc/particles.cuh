@@ -33,6 +33,8 @@ struct ParticleArgs {
     double x0[3];
     double dx, dt;
     int* err;
+    int inline_links;  // 1: rebuild changed link lists here; 0: flag them (relink) for k_links
+    int pad;
     int* nbox_out[2];  // [nparts][6] solid boxes (lo, hi) published for the bulk pass two ticks
                        // later (tick update writes [0]; setup writes both); null to skip
 };
@@ -111,6 +113,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty, s_keep;
     __shared__ unsigned long long s_slack;  // bit pattern of a non-negative double
     __shared__ unsigned s_links;
+    __shared__ int s_warp[9];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
     // the particle record is staged in shared memory: the update below is a
     // serial chain of reads and writes that must not go to global memory
@@ -123,11 +126,12 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     }
     __syncthreads();
     ParticleDev& P = sP;
+    if (tid == 0) P.relink = 0;  // set again below when this update changes the intervals
 
     // 1. momentum exchange: fixed-order reduction of the per-chunk partials
     double acc[6] = {0, 0, 0, 0, 0, 0};
     if (a.mode == 0) {
-        const int nch = (near_volume(P, a.g, D) + kFixBlock - 1) / kFixBlock;
+        const int nch = (P.nlinks + kFixBlock - 1) / kFixBlock;  // chunks of the link list the fix-up ran over
         for (int l = tid; l < nch; l += blockDim.x) {
             const double* q = a.partial + (long long)(P.part_off + l) * kPartialStride;
             for (int k = 0; k < 6; ++k) acc[k] += q[k];
@@ -376,6 +380,91 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     }
     __syncthreads();
 
+    // 4b. the boundary-link list the next fix-up runs over: fluid nodes x of
+    //     the near box with mask bit j set where x - c_j is solid.  Rebuilt
+    //     only when the intervals changed: here, row by row of the near box
+    //     (one CTA; fine for small particles), or flagged for k_links_count
+    //     and k_links_write (a grid over the near box).
+    if (s_changed && !a.inline_links && tid == 0) P.relink = 1;
+    if (s_changed && a.inline_links) {
+        const int ex = near_extent(P, a.g, 0, D), ey = near_extent(P, a.g, 1, D), ez = near_extent(P, a.g, 2, D);
+        const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+        const int nrows = (P.slo[0] > P.shi[0] || P.slo[1] > P.shi[1] || P.slo[2] > P.shi[2]) ? 0 : ey * ez;
+        // interval of row (y, z) of the solid box, or empty
+        auto row_ivl = [&](int y, int z) -> int2 {
+            if (y < P.slo[1] || y > P.shi[1] || z < P.slo[2] || z > P.shi[2]) return make_int2(1, 0);
+            const int r = (y - P.slo[1]) + (P.shi[1] - P.slo[1] + 1) * (z - P.slo[2]);
+            return ivl_smem ? s_ivl[r] : a.ivl[P.ivl_off + r];
+        };
+        // the links of near-box row rr, counted or written from `out`
+        auto scan_row = [&](int rr, int2* out) -> int {
+            const int y = wrap_idx(P.slo[1] - 1 + rr % ey, ny);
+            const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + rr / ey, nz) : 0;
+            int2 nb[9];
+            int nn = 0;
+            for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); ++dz)
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int2 iv = row_ivl(wrap_idx(y + dy, ny), D == 3 ? wrap_idx(z + dz, nz) : 0);
+                    if (iv.x <= iv.y) nb[nn++] = iv;
+                }
+            if (nn == 0) return 0;
+            int cnt = 0;
+#pragma unroll 1
+            for (int rx = 0; rx < ex; ++rx) {
+                const int x = wrap_idx(P.slo[0] - 1 + rx, nx);
+                const int xm = wrap_idx(x - 1, nx), xp = wrap_idx(x + 1, nx);
+                bool cand = false;
+                for (int k = 0; k < nn; ++k)
+                    cand = cand || (x >= nb[k].x && x <= nb[k].y) || (xm >= nb[k].x && xm <= nb[k].y) ||
+                           (xp >= nb[k].x && xp <= nb[k].y);
+                if (!cand || inS(x, y, z)) continue;
+                unsigned mask = 0;
+                for (int j = 1; j < L::Q; ++j) {
+                    const int i = L::opp(j);  // source x - c_j = x + c_i
+                    if (inS(wrap_idx(x + L::cx(i), nx), wrap_idx(y + L::cy(i), ny), wrap_idx(z + L::cz(i), nz)))
+                        mask |= 1u << j;
+                }
+                if (!mask) continue;
+                if (out) out[cnt] = make_int2(x + nx * (y + ny * z), (int)mask);
+                ++cnt;
+            }
+            return cnt;
+        };
+        int base = 0;
+        for (int r0 = 0; r0 < nrows; r0 += blockDim.x) {
+            const int rr = r0 + tid;
+            const int c = rr < nrows ? scan_row(rr, nullptr) : 0;
+            // exclusive prefix of the counts over the CTA
+            const int lane = tid & 31, warp = tid >> 5;
+            int v = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (lane == 31) s_warp[warp] = v;
+            __syncthreads();
+            if (tid == 0) {
+                int run = 0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                    const int t = s_warp[w];
+                    s_warp[w] = run;
+                    run += t;
+                }
+                s_warp[8] = run;
+            }
+            __syncthreads();
+            const int off = base + s_warp[warp] + v - c;
+            if (c > 0) {
+                if (off + c <= P.link_cap) scan_row(rr, a.links + P.link_off + off);
+                else atomicOr(a.err, kErrLinkOverflow);
+            }
+            base += s_warp[8];
+            __syncthreads();
+        }
+        if (tid == 0) P.nlinks = base < P.link_cap ? base : P.link_cap;
+    }
+    __syncthreads();
+
     // 5. candidate bits of the tiles around the particle
     bool same = true;
     for (int k = 0; k < 6; ++k) same = same && s_oldbox[k] == s_newbox[k];
@@ -396,6 +485,88 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
 template <class L>
 __global__ void __launch_bounds__(kPartBlock) k_particles(const ParticleArgs a) {
     particles_body<L>(a, a.mode != 0 ? a.setup_pid : (int)blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Link-list rebuild for particles flagged by the particle update, in two
+// passes over the near box (one thread per node, blocks_per_particle CTAs per
+// particle): k_links_count stores each CTA's number of link nodes, then
+// k_links_write places each CTA's link nodes, in node order, after those of
+// the CTAs before it.  The list comes out in near-box order whatever the
+// scheduling, so the fix-up's chunks and FP64 partial sums are reproducible.
+// ---------------------------------------------------------------------------
+constexpr int kLinkBlock = 256;
+
+// the mask of near-box node v of particle P (0: not a link node)
+template <class L>
+__device__ __forceinline__ unsigned near_node_mask(const ParticleArgs& a, const ParticleDev& P, int v, int* cell) {
+    constexpr int Q = L::Q, D = L::D;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int e0 = near_extent(P, a.g, 0, D), e1 = near_extent(P, a.g, 1, D);
+    const int x = wrap_idx(P.slo[0] - 1 + v % e0, nx);
+    const int y = wrap_idx(P.slo[1] - 1 + (v / e0) % e1, ny);
+    const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + v / (e0 * e1), nz) : 0;
+    *cell = x + nx * (y + ny * z);
+    if (solid_at(P, a.ivl, x, y, z)) return 0u;
+    unsigned mask = 0;
+#pragma unroll
+    for (int j = 1; j < Q; ++j) {
+        const int i = L::opp(j);  // source x - c_j = x + c_i
+        if (solid_at(P, a.ivl, wrap_idx(x + L::cx(i), nx), wrap_idx(y + L::cy(i), ny), wrap_idx(z + L::cz(i), nz)))
+            mask |= 1u << j;
+    }
+    return mask;
+}
+
+template <class L>
+__global__ void __launch_bounds__(kLinkBlock) k_links_count(const ParticleArgs a, int bpp, int* counts) {
+    __shared__ int s_w[kLinkBlock / 32];
+    const int p = blockIdx.x / bpp, chunk = blockIdx.x % bpp;
+    const ParticleDev& P = a.parts[p];
+    if (!P.relink) return;
+    const int v = chunk * kLinkBlock + threadIdx.x;
+    int cell = 0;
+    const bool link = v < near_volume(P, a.g, L::D) && near_node_mask<L>(a, P, v, &cell) != 0u;
+    const unsigned bal = __ballot_sync(0xffffffffu, link);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int w = 0; w < kLinkBlock / 32; ++w) c += s_w[w];
+        counts[blockIdx.x] = c;
+    }
+}
+
+template <class L>
+__global__ void __launch_bounds__(kLinkBlock) k_links_write(const ParticleArgs a, int bpp, const int* counts) {
+    __shared__ int s_w[kLinkBlock / 32];
+    __shared__ int s_base;
+    const int p = blockIdx.x / bpp, chunk = blockIdx.x % bpp;
+    ParticleDev* G = a.parts + p;
+    const ParticleDev& P = *G;
+    if (!P.relink) return;
+    if (threadIdx.x == 0) {
+        int base = 0, total = 0;
+        for (int c = 0; c < bpp; ++c) {
+            if (c == chunk) base = total;
+            total += counts[p * bpp + c];
+        }
+        s_base = base;
+        if (chunk == 0) G->nlinks = total < P.link_cap ? total : P.link_cap;
+        if (total > P.link_cap) atomicOr(a.err, kErrLinkOverflow);
+    }
+    const int v = chunk * kLinkBlock + threadIdx.x;
+    int cell = 0;
+    const unsigned mask = v < near_volume(P, a.g, L::D) ? near_node_mask<L>(a, P, v, &cell) : 0u;
+    const bool link = mask != 0u;
+    const unsigned bal = __ballot_sync(0xffffffffu, link);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_w[warp] = __popc(bal);
+    __syncthreads();
+    int off = s_base;
+    for (int w = 0; w < warp; ++w) off += s_w[w];
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (link && off < P.link_cap) a.links[P.link_off + off] = make_int2(cell, (int)mask);
 }
 
 }  // namespace lbm
