@@ -31,6 +31,7 @@ namespace lbm {
 constexpr int kBlock = 256;        // threads per CTA of the scalar kernels
 constexpr int kFixBlock = 64;      // link entries per fix-up CTA
 constexpr int kPartialStride = 8;  // doubles per partial-sum slot (F[3], T[3], pad)
+constexpr int kLinkOcParams = 8;   // particles whose (link_off, link_cap) the fix-up gets as parameters
 
 // device error word bits
 constexpr int kErrLinkOverflow = 1;
@@ -88,6 +89,8 @@ struct StepArgs {
     const int* wnodes;                    // wall nodes (static)
     int nwlinks, nwnodes;
     int maxchunks;                        // fix-up CTAs reserved per particle
+    int nlinkoc;                          // particles [0, nlinkoc) have linkoc filled (0: read the records)
+    int linkoc[kLinkOcParams][2];         // (link_off, link_cap) of the first particles (static)
     int vrows;                            // x-rows per tile of the vector bulk pass
     long long vtiles;                     // tiles of the vector bulk pass
     int vnt1;                             // vector tiles per z-slice

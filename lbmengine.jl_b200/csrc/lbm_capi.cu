@@ -249,6 +249,11 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.nwlinks = h->nwlinks;
     a.nwnodes = h->nwnodes;
     a.maxchunks = h->maxchunks;
+    a.nlinkoc = (int)std::min<size_t>(h->hparts.size(), kLinkOcParams);
+    for (int p = 0; p < a.nlinkoc; ++p) {
+        a.linkoc[p][0] = h->hparts[p].link_off;
+        a.linkoc[p][1] = h->hparts[p].link_cap;
+    }
     a.vrows = h->vrows;
     a.vnt1 = h->vnt1;
     a.vtiles = h->vtiles;

@@ -48,7 +48,7 @@ struct OpsImpl {
         k_bulk<L, ST, TRT><<<grid, block, 0, s>>>(a);
     }
     static void fixup(const StepArgs& a, unsigned grid, cudaStream_t s) {
-        k_fixup<L, ST, TRT><<<grid, kFixBlock, 0, s>>>(a);
+        k_fixup<L, ST, TRT><<<grid, kFixThreads, 0, s>>>(a);
     }
     static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
         k_particles<L><<<grid, kPartBlock, 0, s>>>(a);

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
         } else if (t < nab) {
             cta_wait(&q->cnt_a, (int)it.na, err);
             const int2 m = it.bmap[t - it.na];
-            fixup_body<L, ST, TRT>(args[m.x], m.y);
+            fixup_body<L, ST, TRT, kTickBlock>(args[m.x], m.y);
             cta_done(&q->cnt_b);
         } else if (t < nabc) {
             cta_wait(&q->cnt_b, (int)it.nb, err);
