@@ -24,16 +24,46 @@
 
 namespace lbm {
 
-constexpr int kFixCoord = 64;     // near-box node coordinates staged per axis
 constexpr int kFixThreads = 256;  // threads of a k_fixup CTA
+
+// Ladd term and momentum exchange of one link slot (fluids.jl:176-205) for
+// particle P; v accumulates the slot value, acc the owner's F and T.
+template <int D>
+__device__ __forceinline__ void ladd_link(const StepArgs& a, const ParticleDev& P, bool owner, int ci0, int ci1,
+                                          int ci2, const double* Tc, const double* Xc, double rhoL, double gi,
+                                          double wi, double& v, double* acc) {
+    double up[3];
+    slip_velocity<D>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, Tc[0], Tc[1], Tc[2], up);
+    v += 6.0 * rhoL * (-(ci0 * up[0] + ci1 * up[1] + ci2 * up[2]));
+    if (owner && (P.coupleF || P.coupleT)) {
+        // f*_i(x) + f_j(x) in f units; F -= coeff*s*c_j = coeff*s*c_i
+        const double cs = a.coeff * (wi * (2.0 * a.rho0 + gi + v));
+        if (P.coupleF) {
+            acc[0] += cs * ci0;
+            acc[1] += cs * ci1;
+            acc[2] += cs * ci2;
+        }
+        if (P.coupleT) {  // T -= coeff*cross(s*(x-R), c_j) = coeff*cross(s*(x-R), c_i)
+            const double r0 = Xc[0] - P.mR[0], r1 = Xc[1] - P.mR[1], r2 = D == 3 ? Xc[2] - P.mR[2] : 0.0;
+            if (D == 2) {
+                acc[3] += cs * (r0 * ci1 - r1 * ci0);
+            } else {
+                acc[3] += cs * (r1 * ci2 - r2 * ci1);
+                acc[4] += cs * (-r0 * ci2 + r2 * ci0);
+                acc[5] += cs * (r0 * ci1 - r1 * ci0);
+            }
+        }
+    }
+}
 
 // One CTA per kFixBlock link entries, NT threads (NT >= kFixBlock).
 //   round 1: the particle record, the entry (cell, mask) of threads < kFixBlock
 //            ((link_off, link_cap) of the first particles come with the
 //            kernel parameters, so the entry load does not wait for the record)
-//   round 2: the owner's near-box coordinates, the entries' populations,
-//            collided once per entry into shared memory; the links of all
-//            entries are listed (entry, j) in shared memory
+//   round 2: each entry's populations and the coordinates of its node and of
+//            the node's +-1 neighbours per axis (every link target x + c_i is
+//            among them); the node is collided once into shared memory and
+//            the links of all entries are listed (entry, j)
 //   links:   the list is spread over all NT threads, one link slot each
 //            (the Ladd terms are FP64 chains with a square root and a
 //            division; one thread per entry would run its links in series)
@@ -52,11 +82,12 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
     __shared__ R s_g[Q][kFixBlock];      // post-collision populations of the entries (f/w - rho0)
     __shared__ double s_rho[kFixBlock];  // rho^n of the entries
     __shared__ int s_cell[kFixBlock];
+    __shared__ int s_xyz[3][kFixBlock];
+    __shared__ double s_C[3][3][kFixBlock];  // coordinate of x-1, x, x+1 per axis
     __shared__ unsigned short s_list[kFixBlock * Q];  // (entry << 5) | j of every link slot
     __shared__ int s_wcnt[2];
     __shared__ double s_red[NT / 32][6];
     __shared__ ParticleDev sP;
-    __shared__ double s_X[3][kFixCoord];
     __shared__ int s_alone;
     const int tid = threadIdx.x;
     const long long npb = (long long)a.nparts * a.maxchunks;
@@ -111,6 +142,23 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
     }
     if (tid == 0) s_alone = 1;
     __syncthreads();
+    // round 2 loads first: populations and coordinates of each entry's node
+    const unsigned mask = valid ? (unsigned)ent.y : 0u;
+    NodeState<L, ST, TRT> st;
+    double cc[3][3];
+    int xyz[3] = {0, 0, 0};
+    if (valid) {
+        const int cell = ent.x;
+        xyz[0] = cell % nx;
+        xyz[1] = (cell / nx) % ny;
+        xyz[2] = cell / (nx * ny);
+        load_pops<L, ST>(a, cell, true, st.g);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int o = 0; o < 3; ++o)
+                cc[k][o] = k < D ? a.coord[k][wrap_idx(xyz[k] + o - 1, a.g.n[k])] : 0.0;
+    }
     // break rule of the Ladd loop (fluids.jl:184): for streaming direction j
     // only particles before the first one without links in j contribute.
     // The owner is "alone" when no other particle's near box meets its own:
@@ -137,25 +185,19 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         }
     }
     if (is_part && a.wall && tid == 0) s_alone = 0;
-    // the owner's near-box coordinates (one load per thread and axis)
-    int ext[3] = {1, 1, 1};
-    if (is_part)
-        for (int k = 0; k < D; ++k) ext[k] = near_extent(sP, a.g, k, D);
-    const bool cst = is_part && ext[0] <= kFixCoord && ext[1] <= kFixCoord && ext[2] <= kFixCoord;
-    if (cst)
-        for (int s = tid; s < D * kFixCoord; s += NT) {
-            const int k = s / kFixCoord, i = s - k * kFixCoord;
-            if (i < ext[k]) s_X[k][i] = a.coord[k][wrap_idx(sP.slo[k] - 1 + i, a.g.n[k])];
-        }
     // collide each entry's node once
-    const unsigned mask = valid ? (unsigned)ent.y : 0u;
     if (valid) {
-        NodeState<L, ST, TRT> st;
-        load_collide<L, ST, TRT>(a, ent.x, true, st);
+        st.rho = collide_node<L, ST, TRT>(a, ent.x, true, st.g);
         s_rho[tid] = (double)st.rho;  // rho^n(x), the density of model.massDensity
         s_cell[tid] = ent.x;
 #pragma unroll
         for (int i = 0; i < Q; ++i) s_g[i][tid] = st.g[i] * R(a.inv_scale);  // storage -> f/w - rho0
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            s_xyz[k][tid] = xyz[k];
+#pragma unroll
+            for (int o = 0; o < 3; ++o) s_C[k][o][tid] = cc[k][o];
+        }
     }
     // list the link slots: entries 0..31 and 32..63 scan their counts per warp
     int off = 0;
@@ -178,77 +220,48 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         for (unsigned m = mask; m; m &= m - 1) s_list[off++] = (unsigned short)((tid << 5) | (__ffs(m) - 1));
     }
     __syncthreads();
-    // coordinate of node index i on axis k (staged for the owner's near box)
-    auto coordf = [&](int k, int i) -> double {
-        return cst ? s_X[k][wrap_idx(i - (sP.slo[k] - 1), a.g.n[k])] : a.coord[k][i];
-    };
-    const double rho0 = a.rho0;
     const bool alone = is_part && s_alone;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int l = tid; l < nlist; l += NT) {
         const int item = s_list[l];
         const int el = item >> 5, j = item & 31;
         const int cell = s_cell[el];
-        const int x = cell % nx, y = (cell / nx) % ny, z = cell / (nx * ny);
         const int i = s_lat[3][j];  // x - c_j = x + c_i is the solid source node
         const int ci0 = s_lat[0][i], ci1 = s_lat[1][i], ci2 = s_lat[2][i];
         R vout;
         if (a.wall && a.wall[cell]) {
-            vout = R(-rho0);  // wall nodes hold f = 0 (fluids.jl:154)
+            vout = R(-a.rho0);  // wall nodes hold f = 0 (fluids.jl:154)
         } else {
-            const int tx = wrap_idx(x + ci0, nx), ty = wrap_idx(y + ci1, ny), tz = wrap_idx(z + ci2, nz);
-            const int t = tx + nx * (ty + ny * tz);
+            const int x = s_xyz[0][el], y = s_xyz[1][el], z = s_xyz[2][el];
             const double rhoL = s_rho[el];
             const double gi = (double)s_g[i][el];
+            const double wi = s_w[i];
+            const double Tc[3] = {s_C[0][1 + ci0][el], s_C[1][1 + ci1][el], D == 3 ? s_C[2][1 + ci2][el] : 0.0};
+            const double Xc[3] = {s_C[0][1][el], s_C[1][1][el], D == 3 ? s_C[2][1][el] : 0.0};
             double v = gi;  // halfway bounce-back: f_j(x) = f*_i(x)
-            if (a.uw) {     // moving walls (fluids.jl:168-174)
+            const int tx = wrap_idx(x + ci0, nx), ty = wrap_idx(y + ci1, ny), tz = wrap_idx(z + ci2, nz);
+            if (a.uw) {  // moving walls (fluids.jl:168-174)
+                const long long t = tx + (long long)nx * (ty + (long long)ny * tz);
                 const double dot = -(ci0 * a.uw[t] + ci1 * a.uw[N + t] + (D == 3 ? ci2 * a.uw[2 * N + t] : 0.0));
                 v += 6.0 * rhoL * dot;
             }
             // Ladd terms (fluids.jl:176-189) of every particle with link (x, j), in order
-            const double T0 = coordf(0, tx), T1 = coordf(1, ty), T2 = D == 3 ? coordf(2, tz) : 0.0;
-            const double wi = s_w[i];
-            const int tile = x / a.g.t[0] + a.g.nt[0] * (y / a.g.t[1] + a.g.nt[1] * (z / a.g.t[2]));
-            int q = alone ? p : -1;
-            const ParticleDev* Pp = alone ? &sP : nullptr;
-            int w = 0;
-            unsigned long long bits = 0;
-            while (true) {
-                if (!alone) {  // next candidate of the tile, in ascending order
+            if (alone) {
+                if (p < s_first[j]) ladd_link<D>(a, sP, true, ci0, ci1, ci2, Tc, Xc, rhoL, gi, wi, v, acc);
+            } else {
+                const int tile = x / a.g.t[0] + a.g.nt[0] * (y / a.g.t[1] + a.g.nt[1] * (z / a.g.t[2]));
+                int w = 0;
+                unsigned long long bits = 0;
+                while (true) {  // candidates of the tile, in ascending order
                     while (bits == 0 && w < a.words) bits = a.tilebits[(long long)tile * a.words + w++];
                     if (bits == 0) break;
-                    q = (w - 1) * 64 + __ffsll((long long)bits) - 1;
+                    const int q = (w - 1) * 64 + __ffsll((long long)bits) - 1;
                     bits &= bits - 1;
-                    Pp = q == p ? &sP : a.parts + q;
+                    if (q >= s_first[j]) break;  // particles are visited in ascending order
+                    const ParticleDev& P = q == p ? sP : a.parts[q];
+                    if (solid_at(P, a.ivl, tx, ty, tz) && !solid_at(P, a.ivl, x, y, z))
+                        ladd_link<D>(a, P, q == p, ci0, ci1, ci2, Tc, Xc, rhoL, gi, wi, v, acc);
                 }
-                if (q >= s_first[j]) break;  // particles are visited in ascending order
-                const ParticleDev& P = *Pp;
-                if (alone || (solid_at(P, a.ivl, tx, ty, tz) && !solid_at(P, a.ivl, x, y, z))) {
-                    double up[3];
-                    slip_velocity<D>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, T0, T1, T2, up);
-                    v += 6.0 * rhoL * (-(ci0 * up[0] + ci1 * up[1] + ci2 * up[2]));
-                    if (q == p && (P.coupleF || P.coupleT)) {
-                        // f*_i(x) + f_j(x) in f units; F -= coeff*s*c_j = coeff*s*c_i
-                        const double cs = a.coeff * (wi * (2.0 * rho0 + gi + v));
-                        if (P.coupleF) {
-                            acc[0] += cs * ci0;
-                            acc[1] += cs * ci1;
-                            acc[2] += cs * ci2;
-                        }
-                        if (P.coupleT) {  // T -= coeff*cross(s*(x-R), c_j) = coeff*cross(s*(x-R), c_i)
-                            const double X0 = coordf(0, x), X1 = coordf(1, y), X2 = D == 3 ? coordf(2, z) : 0.0;
-                            const double r0 = X0 - P.mR[0], r1 = X1 - P.mR[1], r2 = D == 3 ? X2 - P.mR[2] : 0.0;
-                            if (D == 2) {
-                                acc[3] += cs * (r0 * ci1 - r1 * ci0);
-                            } else {
-                                acc[3] += cs * (r1 * ci2 - r2 * ci1);
-                                acc[4] += cs * (-r0 * ci2 + r2 * ci0);
-                                acc[5] += cs * (r0 * ci1 - r1 * ci0);
-                            }
-                        }
-                    }
-                }
-                if (alone) break;
             }
             vout = (R)v;
         }
