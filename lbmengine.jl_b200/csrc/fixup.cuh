@@ -68,6 +68,11 @@ __device__ __forceinline__ void ladd_link(const StepArgs& a, const ParticleDev& 
 //            (the Ladd terms are FP64 chains with a square root and a
 //            division; one thread per entry would run its links in series)
 //   the momentum exchange of the CTA is reduced in a fixed order.
+// Everything before the stores reads only state that the bulk pass of the
+// same tick does not write (source populations, particle records, link
+// lists), so the values are staged in shared memory and stored after
+// grid_dep_wait(): launched with a programmatic edge from the bulk pass, the
+// kernel computes during the bulk pass's last wave.
 template <class L, int ST, bool TRT, int NT>
 __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b) {
     static_assert(NT >= kFixBlock && NT % 32 == 0 && kFixBlock == 64, "fix-up CTA shape");
@@ -85,6 +90,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
     __shared__ int s_xyz[3][kFixBlock];
     __shared__ double s_C[3][3][kFixBlock];  // coordinate of x-1, x, x+1 per axis
     __shared__ unsigned short s_list[kFixBlock * Q];  // (entry << 5) | j of every link slot
+    __shared__ R s_val[kFixBlock * Q];                // the value of each listed slot
     __shared__ int s_wcnt[2];
     __shared__ double s_red[NT / 32][6];
     __shared__ ParticleDev sP;
@@ -99,6 +105,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         const long long k0 = (b - npb - nwlb) * kFixBlock;
         const int n = (int)min((long long)kFixBlock, (long long)a.nwnodes - k0);
         const T z0 = SS::enc(R(-a.rho0), R(a.scale));
+        grid_dep_wait();
         for (int s = tid; s < n * Q; s += NT) dst[(long long)(s % Q) * N + a.wnodes[k0 + s / Q]] = z0;
         return;
     }
@@ -265,7 +272,14 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
             }
             vout = (R)v;
         }
-        dst[j * N + cell] = SS::enc(vout, R(a.scale));
+        s_val[l] = vout;
+    }
+    // the stores, after the bulk pass's stores to the same slots (each thread
+    // stores the slots it computed)
+    grid_dep_wait();
+    for (int l = tid; l < nlist; l += NT) {
+        const int item = s_list[l];
+        dst[(item & 31) * N + s_cell[item >> 5]] = SS::enc(s_val[l], R(a.scale));
     }
     if (!is_part) return;
     // fixed-order reduction: butterfly inside warps, warps summed in order

@@ -120,6 +120,14 @@ struct StepArgs {
 
 __host__ __device__ __forceinline__ int wrap_idx(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// Programmatic dependent launch.  grid_dep_trigger(): once every CTA of this
+// grid has issued it (or exited), a kernel that depends on this one through a
+// programmatic edge may start.  grid_dep_wait(): blocks until the grids this
+// kernel depends on through such an edge have completed and their writes are
+// visible.  Both are no-ops for kernels launched without that dependency.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // getSphere test (src/gpu/kernels.jl:335-353): ((X1-R1)^2 + (X2-R2)^2 [+ (X3-R3)^2]) < r^2,
 // evaluated left to right in FP64 without contraction so that masks are
 // bit-identical to the reference's.  For a fixed (y, z) row the test is
@@ -359,6 +367,7 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
     const int z = bz * a.g.t[2] + threadIdx.z;
     const bool valid = x < nx && y < ny && z < nz;
     const int cell = valid ? x + nx * (y + ny * z) : 0;
+    grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
     NodeState<L, ST, TRT> s;
     load_collide<L, ST, TRT>(a, cell, valid, s);
     if (!valid) return;
@@ -510,6 +519,7 @@ constexpr int bulk_threads_per_sm() { return L::Q <= 9 ? 1024 : 512; }
 template <class L, int ST, bool TRT, int B>
 __global__ void __launch_bounds__(B, bulk_threads_per_sm<L>() / B) k_bulk_v4(const StepArgs a) {
     __shared__ float s_ex[x_moving_dirs<L>()][B];
+    grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
     bulk_v4_tile<L, ST, TRT, B>(a, blockIdx.x, s_ex);
 }
 

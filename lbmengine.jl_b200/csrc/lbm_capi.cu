@@ -447,6 +447,37 @@ void prof_record(lbm_handle* h, int slot, int k, cudaStream_t s) {
         cudaEventRecord(prof_event(h, slot, k), s);
 }
 
+// Inside a stream capture: the single node the next captured work on `s`
+// depends on (null outside a capture or for several).
+cudaGraphNode_t capture_tail(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n = 0;
+    if (cudaStreamGetCaptureInfo_v3(s, &st, nullptr, nullptr, &deps, nullptr, &n) != cudaSuccess) return nullptr;
+    return st == cudaStreamCaptureStatusActive && n == 1 ? deps[0] : nullptr;
+}
+
+// Inside a stream capture: the next captured kernel depends on kernel node
+// `from` through a programmatic edge (its other dependencies stay full ones).
+void programmatic_from(cudaStream_t s, cudaGraphNode_t from) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n = 0;
+    if (cudaStreamGetCaptureInfo_v3(s, &st, nullptr, nullptr, &deps, nullptr, &n) != cudaSuccess ||
+        st != cudaStreamCaptureStatusActive || n > 8)
+        return;
+    cudaGraphNode_t nodes[8];
+    cudaGraphEdgeData edges[8] = {};
+    for (size_t i = 0; i < n; ++i) {
+        nodes[i] = deps[i];
+        if (deps[i] == from) {
+            edges[i].from_port = cudaGraphKernelNodePortProgrammatic;
+            edges[i].type = cudaGraphDependencyTypeProgrammatic;
+        }
+    }
+    cudaStreamUpdateCaptureDependencies_v2(s, nodes, edges, n, cudaStreamSetCaptureDependencies);
+}
+
 // Enqueue one tick (capturable); `slot` selects the profiling events.
 // Persistent tick kernel: one launch.  Otherwise
 //   main: bulk(n) -> [wait particles(n-1)] -> fixup(n) -> bulk(n+1) ...
@@ -463,12 +494,24 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
     const StepArgs a = step_args(h, src);
     launch_bulk(h, a, h->stream);
     prof_record(h, slot, 1, h->stream);
+    // The fix-up follows the bulk pass through a programmatic edge (it computes
+    // during the bulk pass's last wave and stores after it) unless per-kernel
+    // events sit between the two.  Inside a capture the edge is set by hand so
+    // that the one from the particle update stays a full dependency; outside
+    // one the launch attribute serves when no event wait comes between.
+    const bool early = h->profiling < 2;
+    const cudaGraphNode_t bulk_node = early ? capture_tail(h->stream) : nullptr;
+    bool waited = false;
     if (h->part_pending) {
         cudaStreamWaitEvent(h->stream, h->ev_part, 0);
         h->part_pending = false;
+        waited = true;
     }
     const long long nb = fixup_blocks(h);
-    if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
+    if (nb > 0) {
+        if (bulk_node) programmatic_from(h->stream, bulk_node);
+        h->ops.fixup(a, (unsigned)nb, h->stream, early && !bulk_node && !waited);
+    }
     if (a.nparts == 0) prof_record(h, slot, 2, h->stream);
     if (a.nparts > 0) {
         cudaEventRecord(h->ev_fix, h->stream);
@@ -1182,7 +1225,7 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
             launch_bulk(h, a, h->stream);
             b = 1 - b;
         } else if (kernel == LBM_KERNEL_FIXUP) {
-            h->ops.fixup(a, (unsigned)fixup_blocks(h), h->stream);
+            h->ops.fixup(a, (unsigned)fixup_blocks(h), h->stream, false);
         } else if (kernel == LBM_KERNEL_TICK) {
             h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
             b = 1 - b;
@@ -1607,7 +1650,7 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
         const StepArgs a = noalloc_step_args(h, h->cur, scratch);
         pa.nbox_out[0] = h->d_nbox[h->cur];
         launch_bulk(h, a, h->stream);
-        if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream);
+        if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream, false);
         if (np > 0) {
             h->ops.particles(pa, (unsigned)np, h->stream);
             h->ops.links(pa, np, h->link_bpp, h->d_linkcnt, h->stream);
