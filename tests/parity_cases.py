@@ -81,6 +81,15 @@ CASES = {
         particles=[dict(kind="squirmer", radius=3.7, position=[0.2, 0.1, -0.3], swimmingSpeed=2e-3, beta=1.0,
                         coupleForces=True, coupleTorques=True, swimmingDirection=seeded_direction(5, 3))],
         steps=60),
+    # a squirmer whose link list (~2,300 entries) is longer than the 32 fix-up
+    # CTAs of a particle cover in one pass, so each walks several chunks
+    "d3q19_large_squirmer": dict(
+        model=dict(dims=3, velocities="D3Q19", collisionModel="trt", latticeParameter=1.0,
+                   relaxationTimeRatio=0.8, xlims=(-20.0, 19.0)),
+        particles=[dict(kind="squirmer", radius=13.5, position=[0.4, -0.3, 0.2], swimmingSpeed=1e-3, beta=2.0,
+                        coupleForces=True, coupleTorques=True, swimmingDirection=seeded_direction(9, 3),
+                        massDensity=3.0)],
+        steps=30),
     "d2q9_incompressible": dict(
         model=dict(dims=2, latticeParameter=1.0, relaxationTimeRatio=0.8, collisionModel="trt",
                    xlims=(-16.0, 15.0), isFluidCompressible=False, massDensity=1.0,
