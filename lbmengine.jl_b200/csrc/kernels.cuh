@@ -71,6 +71,22 @@ struct ParticleDev {
     int pad1;
 };
 
+// Collision constants in one precision (see collide()), derived on the host
+// from the FP64 fields of StepArgs by fill_collide_consts(), so that no kernel
+// converts them per node.
+template <class R>
+struct CollideK {
+    R S, invS, rho0, hdt, rho_inc;
+    R rest;      // rest population: a* = rest a + e0 (1 - omega+ or 1 - omega)
+    R hsum;      // BGK pairs: a* = hsum a + E + O (1 - omega)
+    R le, lo;    // TRT pairs: a* = le (a + b) + lo (a - b) + E + O ((1 - omega+)/2, (1 - omega-)/2)
+    R omE;       // omega+ (TRT) or omega (BGK): weight of the equilibrium's even part
+    R c45, c3;   // 4.5 omega+ and 3 omega- (TRT), 4.5 omega and 3 omega (BGK)
+    R gK0, gkA, gkB;
+    R F[3];
+    R gA[27], gB[27];
+};
+
 struct StepArgs {
     const void* src;
     void* dst;
@@ -113,10 +129,55 @@ struct StepArgs {
     // the coefficients used when the force is a per-node field
     double gA[27], gB[27];
     double gK0, gkA, gkB;
+    int trt;                              // collision model of the constants below (0 BGK, 1 TRT)
+    CollideK<float> kf;                   // the constants in FP32 and FP64 (fill_collide_consts)
+    CollideK<double> kd;
     // per-direction population planes of src / dst (vector bulk kernel)
     const void* srcq[27];
     void* dstq[27];
 };
+
+template <class R>
+inline void fill_collide_k(const StepArgs& a, CollideK<R>& k) {
+    k.S = R(a.scale);
+    k.invS = R(a.inv_scale);
+    k.rho0 = R(a.rho0);
+    k.hdt = R(a.half_dt);
+    k.rho_inc = R(a.rho_inc);
+    const double omE = a.trt ? a.omega_p : a.omega;
+    const double omO = a.trt ? a.omega_m : a.omega;
+    k.rest = R(1.0 - omE);
+    k.hsum = R(1.0 - a.omega);
+    k.le = R(0.5 * (1.0 - omE));
+    k.lo = R(0.5 * (1.0 - omO));
+    k.omE = R(omE);
+    k.c45 = R(4.5 * omE);
+    k.c3 = R(3.0 * omO);
+    k.gK0 = R(a.gK0);
+    k.gkA = R(a.gkA);
+    k.gkB = R(a.gkB);
+    for (int i = 0; i < 3; ++i) k.F[i] = R(a.F[i]);
+    for (int i = 0; i < 27; ++i) {
+        k.gA[i] = R(a.gA[i]);
+        k.gB[i] = R(a.gB[i]);
+    }
+}
+
+// derive kf / kd from the FP64 fields (after they are set)
+inline void fill_collide_consts(StepArgs& a) {
+    fill_collide_k(a, a.kf);
+    fill_collide_k(a, a.kd);
+}
+
+template <class R>
+__device__ __forceinline__ const CollideK<R>& collide_k(const StepArgs& a);
+template <>
+__device__ __forceinline__ const CollideK<float>& collide_k<float>(const StepArgs& a) { return a.kf; }
+template <>
+__device__ __forceinline__ const CollideK<double>& collide_k<double>(const StepArgs& a) { return a.kd; }
+
+__device__ __forceinline__ float recip(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 
 __host__ __device__ __forceinline__ int wrap_idx(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
@@ -223,81 +284,77 @@ __device__ __forceinline__ void slip_velocity(const double* sR, const double* sV
 //                TRT  even K0 + B_i cu (k = k+), odd A_i (k = k-)
 // A_i, B_i (and the K0 coefficient) arrive pre-multiplied by S.  For a pair
 // (i, opp(i)) = (a, b) the update is
-//   TRT: a* = (1-h+-h-) a + (h- - h+) b + E + O,  b* = (1-h+-h-) b + (h- - h+) a + E - O
-//   BGK: a* = (1-w) a + E + O,                    b* = (1-w) b + E - O
-// with E the even part (relaxed symmetric equilibrium + even Guo term) and O
-// the odd part, h+- = omega+-/2.
+//   TRT: a* = le (a+b) + lo (a-b) + E + O,  b* = le (a+b) - lo (a-b) + E - O
+//   BGK: a* = (1-w) a + E + O,              b* = (1-w) b + E - O
+// with E the even part (relaxed symmetric equilibrium + even Guo term), O
+// the odd part and le = (1 - omega+)/2, lo = (1 - omega-)/2; the moments are
+// summed from the same pair sums and differences.
 // ---------------------------------------------------------------------------
 template <class L, class R, bool TRT>
 __device__ __forceinline__ R collide(const StepArgs& a, R* g, R Fx, R Fy, R Fz, bool field) {
     constexpr int Q = L::Q;
+    const CollideK<R>& k = collide_k<R>(a);
+    // moments from the pair sums s = a + b and differences d = a - b of each
+    // pair (a, b) = (g_i, g_opp(i)), i < opp(i)
+    R s[Q], d[Q];
     R drho = 0, jx = 0, jy = 0, jz = 0;  // S (rho - rho0), S (j - dt/2 F)
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-        drho = fma(R(L::w(i)), g[i], drho);
-        if (L::cx(i) != 0) jx = fma(R(L::w(i) * L::cx(i)), g[i], jx);
-        if (L::cy(i) != 0) jy = fma(R(L::w(i) * L::cy(i)), g[i], jy);
-        if (L::cz(i) != 0) jz = fma(R(L::w(i) * L::cz(i)), g[i], jz);
+        const int ib = L::opp(i);
+        if (ib < i) continue;
+        if (ib == i) {
+            drho = fma(R(L::w(i)), g[i], drho);
+            continue;
+        }
+        s[i] = g[i] + g[ib];
+        d[i] = g[i] - g[ib];
+        drho = fma(R(L::w(i)), s[i], drho);
+        if (L::cx(i) != 0) jx = fma(R(L::w(i) * L::cx(i)), d[i], jx);
+        if (L::cy(i) != 0) jy = fma(R(L::w(i) * L::cy(i)), d[i], jy);
+        if (L::cz(i) != 0) jz = fma(R(L::w(i) * L::cz(i)), d[i], jz);
     }
-    const R S = R(a.scale), invS = R(a.inv_scale);
-    const R rho = fma(drho, invS, R(a.rho0));
-    const R hdt = R(a.half_dt);
-    jx = fma(jx, invS, hdt * Fx);
-    jy = fma(jy, invS, hdt * Fy);
-    jz = fma(jz, invS, hdt * Fz);
+    const R rho = fma(drho, k.invS, k.rho0);
+    jx = fma(jx, k.invS, k.hdt * Fx);
+    jy = fma(jy, k.invS, k.hdt * Fy);
+    jz = fma(jz, k.invS, k.hdt * Fz);
     R ux = 0, uy = 0, uz = 0;
     if (rho != R(0)) {  // findFluidVelocity: u = 0 where rho == 0
-        const R inv = R(1) / rho;
+        const R inv = recip(rho);
         ux = jx * inv;
         uy = jy * inv;
         uz = jz * inv;
     }
     const R usq = ux * ux + uy * uy + uz * uz;
     const R uF = ux * Fx + uy * Fy + uz * Fz;
-    const R Srq = S * (a.incompressible ? R(a.rho_inc) : rho);
+    const R Srq = k.S * (a.incompressible ? k.rho_inc : rho);
     const R E0 = fma(R(-1.5) * Srq, usq, drho);  // S (g_eq even part at cu = 0)
-    const R K0 = R(a.gK0) * uF;
-    const R kA = R(a.gkA), kB = R(a.gkB);
-    R hsum, hdif, e0, k45, k3;  // pair coefficients
-    if (TRT) {
-        const R omp = R(a.omega_p), omm = R(a.omega_m);
-        hsum = R(1) - R(0.5) * (omp + omm);
-        hdif = R(0.5) * (omm - omp);
-        e0 = fma(omp, E0, K0);
-        k45 = omp * R(4.5) * Srq;
-        k3 = omm * R(3) * Srq;
-    } else {
-        const R om = R(a.omega);
-        hsum = R(1) - om;
-        hdif = R(0);
-        e0 = fma(om, E0, K0);
-        k45 = om * R(4.5) * Srq;
-        k3 = om * R(3) * Srq;
-    }
+    const R e0 = fma(k.omE, E0, k.gK0 * uF);
+    const R k45 = k.c45 * Srq, k3 = k.c3 * Srq;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int ib = L::opp(i);
         if (ib < i) continue;
         if (ib == i) {  // rest direction: a* = (1 - omega+) a + e0
-            g[i] = fma(TRT ? R(1) - R(a.omega_p) : hsum, g[i], e0);
+            g[i] = fma(k.rest, g[i], e0);
             continue;
         }
         const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-        R A = R(a.gA[i]), B = R(a.gB[i]);
+        R A = k.gA[i], B = k.gB[i];
         if (field) {
             const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-            A = kA * cF;
-            B = kB * cF;
+            A = k.gkA * cF;
+            B = k.gkB * cF;
         }
         const R E = fma(fma(k45, cu, B), cu, e0);
         const R O = fma(k3, cu, A);
-        const R ga = g[i], gb = g[ib];
         if (TRT) {
-            g[i] = fma(hsum, ga, fma(hdif, gb, E + O));
-            g[ib] = fma(hsum, gb, fma(hdif, ga, E - O));
+            const R es = fma(k.le, s[i], E), od = fma(k.lo, d[i], O);
+            g[i] = es + od;
+            g[ib] = es - od;
         } else {
-            g[i] = fma(hsum, ga, E + O);
-            g[ib] = fma(hsum, gb, E - O);
+            const R ga = g[i], gb = g[ib];
+            g[i] = fma(k.hsum, ga, E + O);
+            g[ib] = fma(k.hsum, gb, E - O);
         }
     }
     return rho;
@@ -330,9 +387,10 @@ __device__ __forceinline__ typename Store<ST>::R collide_node(const StepArgs& a,
     const long long N = a.g.N;
     R Fx = 0, Fy = 0, Fz = 0;
     if (a.force_mode == 1) {
-        Fx = R(a.F[0]);
-        Fy = R(a.F[1]);
-        Fz = R(a.F[2]);
+        const CollideK<R>& k = collide_k<R>(a);
+        Fx = k.F[0];
+        Fy = k.F[1];
+        Fz = k.F[2];
     } else if (a.force_mode == 2 && valid) {
         Fx = R(a.ffield[cell]);
         Fy = R(a.ffield[N + cell]);
@@ -479,7 +537,7 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
         g[2][i] = v[2];
         g[3][i] = v[3];
     }
-    const R Fx = R(a.F[0]), Fy = R(a.F[1]), Fz = R(a.F[2]);
+    const R Fx = a.kf.F[0], Fy = a.kf.F[1], Fz = a.kf.F[2];
 #pragma unroll
     for (int k = 0; k < 4; ++k) collide<L, R, TRT>(a, g[k], Fx, Fy, Fz, false);
     // the value of each +-x direction that leaves this thread's 4-node segment

@@ -297,6 +297,8 @@ StepArgs step_args(const lbm_handle* h, int src) {
         a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
         a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
     }
+    a.trt = h->trt;
+    fill_collide_consts(a);
     return a;
 }
 
@@ -1614,6 +1616,8 @@ StepArgs noalloc_step_args(const lbm_handle* h, int src, double* partial) {
         a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
         a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
     }
+    a.trt = h->trt;
+    fill_collide_consts(a);
     return a;
 }
 
