@@ -519,9 +519,9 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
         cudaEventRecord(h->ev_fix, h->stream);
         cudaStreamWaitEvent(h->side, h->ev_fix, 0);
         prof_record(h, slot, 2, h->side);
-        const ParticleArgs pa = particle_args(h, 0, 0, src);
+        ParticleArgs pa = particle_args(h, 0, 0, src);
+        pa.inline_links = 1;
         h->ops.particles(pa, (unsigned)a.nparts, h->side);
-        h->ops.links(pa, a.nparts, h->link_bpp, h->d_linkcnt, h->side);
         prof_record(h, slot, 3, h->side);
         cudaEventRecord(h->ev_part, h->side);
         h->part_pending = true;

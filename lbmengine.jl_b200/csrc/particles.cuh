@@ -382,9 +382,10 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
 
     // 4b. the boundary-link list the next fix-up runs over: fluid nodes x of
     //     the near box with mask bit j set where x - c_j is solid.  Rebuilt
-    //     only when the intervals changed: here, row by row of the near box
-    //     (one CTA; fine for small particles), or flagged for k_links_count
-    //     and k_links_write (a grid over the near box).
+    //     only when the intervals changed: here, one near-box row per thread
+    //     from the rows' intervals (the stream schedule and the persistent
+    //     tick kernel), or flagged for k_links_count and k_links_write (a grid
+    //     over the near box).
     if (s_changed && !a.inline_links && tid == 0) P.relink = 1;
     if (s_changed && a.inline_links) {
         const int ex = near_extent(P, a.g, 0, D), ey = near_extent(P, a.g, 1, D), ez = near_extent(P, a.g, 2, D);
@@ -430,10 +431,68 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             }
             return cnt;
         };
+        // Fast form (the near box narrower than the x axis by two): in x' = x - s0
+        // coordinates every row interval lies in [1, ex - 2], so node x' of a row
+        // has a solid source x + c_i exactly when x' + c_i,x lies in the
+        // interval of row (y + c_i,y, z + c_i,z); the candidates are the span
+        // of those shifted intervals outside the row's own one.  Everything is
+        // held in registers (an indexed local array would sit in L1, which the
+        // bulk pass running beside this kernel evicts).
+        const int s0 = P.slo[0] - 1;
+        const bool fast = ex + 2 <= nx;
+        auto row_links = [&](int rr, int2* out) -> int {
+            const int y = wrap_idx(P.slo[1] - 1 + rr % ey, ny);
+            const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + rr / ey, nz) : 0;
+            int lo[3][3], hi[3][3];
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    lo[dy][dz] = 1;
+                    hi[dy][dz] = 0;
+                    if (D == 2 && dz != 1) continue;
+                    const int2 iv = row_ivl(wrap_idx(y + dy - 1, ny), D == 3 ? wrap_idx(z + dz - 1, nz) : 0);
+                    if (iv.x <= iv.y) {
+                        lo[dy][dz] = iv.x - s0;
+                        hi[dy][dz] = iv.y - s0;
+                    }
+                }
+            int cl = ex, ch = -1;
+#pragma unroll
+            for (int i = 1; i < L::Q; ++i) {
+                const int dy = L::cy(i) + 1, dz = L::cz(i) + 1;
+                if (lo[dy][dz] <= hi[dy][dz]) {
+                    cl = min(cl, lo[dy][dz] - L::cx(i));
+                    ch = max(ch, hi[dy][dz] - L::cx(i));
+                }
+            }
+            cl = max(cl, 0);
+            ch = min(ch, ex - 1);
+            const int o0 = lo[1][1], o1 = hi[1][1];  // the row's own solid interval
+            int cnt = 0;
+            for (int xr = cl; xr <= ch; ++xr) {
+                if (xr >= o0 && xr <= o1) {
+                    xr = o1;
+                    continue;
+                }
+                unsigned mask = 0;
+#pragma unroll
+                for (int j = 1; j < L::Q; ++j) {
+                    const int i = L::opp(j);  // source x - c_j = x + c_i
+                    const int dy = L::cy(i) + 1, dz = L::cz(i) + 1;
+                    const int t = xr + L::cx(i);
+                    if (t >= lo[dy][dz] && t <= hi[dy][dz]) mask |= 1u << j;
+                }
+                if (!mask) continue;
+                if (out) out[cnt] = make_int2(wrap_idx(s0 + xr, nx) + nx * (y + ny * z), (int)mask);
+                ++cnt;
+            }
+            return cnt;
+        };
         int base = 0;
         for (int r0 = 0; r0 < nrows; r0 += blockDim.x) {
             const int rr = r0 + tid;
-            const int c = rr < nrows ? scan_row(rr, nullptr) : 0;
+            const int c = rr < nrows ? (fast ? row_links(rr, nullptr) : scan_row(rr, nullptr)) : 0;
             // exclusive prefix of the counts over the CTA
             const int lane = tid & 31, warp = tid >> 5;
             int v = c;
@@ -455,7 +514,10 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             __syncthreads();
             const int off = base + s_warp[warp] + v - c;
             if (c > 0) {
-                if (off + c <= P.link_cap) scan_row(rr, a.links + P.link_off + off);
+                if (off + c <= P.link_cap) {
+                    if (fast) row_links(rr, a.links + P.link_off + off);
+                    else scan_row(rr, a.links + P.link_off + off);
+                }
                 else atomicOr(a.err, kErrLinkOverflow);
             }
             base += s_warp[8];
