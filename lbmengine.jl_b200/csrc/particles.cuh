@@ -15,6 +15,7 @@
 namespace lbm {
 
 constexpr int kIvlSmem = 512;  // rows of solid intervals staged in shared memory
+constexpr int kXSmem = 256;    // x coordinates of the solid box staged in shared memory
 constexpr int kPartBlock = 256;  // CTA size of the stand-alone particle kernel
 
 struct ParticleArgs {
@@ -115,6 +116,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     __shared__ unsigned s_links;
     __shared__ int s_warp[9];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
+    __shared__ double s_xc[kXSmem];   // x coordinates of the solid box (interval rebuild)
     // the particle record is staged in shared memory: the update below is a
     // serial chain of reads and writes that must not go to global memory
     __shared__ ParticleDev sP;
@@ -302,15 +304,25 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     {
         const int lx0 = P.slo[0], lx1 = P.shi[0];
         const int ly = P.shi[1] - P.slo[1] + 1;
+        // the row loop below reads every x coordinate of the box once per row:
+        // from shared memory (global loads there would each wait out the
+        // memory latency of the bulk pass running beside this kernel)
+        const bool xs = lx1 - lx0 + 1 <= kXSmem;
+        if (xs)
+            for (int i = tid; i <= lx1 - lx0; i += blockDim.x) s_xc[i] = a.coord[0][lx0 + i];
+        __syncthreads();
         int changed = 0;
         for (int r = tid; r < s_rows; r += blockDim.x) {
             const int y = P.slo[1] + r % ly;
             const int z = P.slo[2] + r / ly;
+            // the row's global loads first, so that their latencies overlap
+            int2* slot = a.ivl + P.ivl_off + r;
+            const int2 old = *slot;
             const double Y = a.coord[1][y], Z = D == 3 ? a.coord[2][z] : 0.0;
             int xlo = 1, xhi = 0;
             double slack = 1e300;
             for (int x = lx0; x <= lx1; ++x) {
-                const double d2 = sphere_d2<D>(a.coord[0][x], Y, Z, P.vR);
+                const double d2 = sphere_d2<D>(xs ? s_xc[x - lx0] : a.coord[0][x], Y, Z, P.vR);
                 if (d2 < P.r2) {
                     if (xlo > xhi) xlo = x;
                     xhi = x;
@@ -319,8 +331,6 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             }
             // non-negative doubles order like their bit patterns
             atomicMin(&s_slack, (unsigned long long)__double_as_longlong(slack));
-            int2* slot = a.ivl + P.ivl_off + r;
-            const int2 old = *slot;
             if (old.x != xlo || old.y != xhi) changed = 1;
             *slot = make_int2(xlo, xhi);
             if (r < kIvlSmem) s_ivl[r] = make_int2(xlo, xhi);
@@ -443,32 +453,41 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
         auto row_links = [&](int rr, int2* out) -> int {
             const int y = wrap_idx(P.slo[1] - 1 + rr % ey, ny);
             const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + rr / ey, nz) : 0;
-            int lo[3][3], hi[3][3];
-#pragma unroll
-            for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-                for (int dy = 0; dy < 3; ++dy) {
-                    lo[dy][dz] = 1;
-                    hi[dy][dz] = 0;
-                    if (D == 2 && dz != 1) continue;
-                    const int2 iv = row_ivl(wrap_idx(y + dy - 1, ny), D == 3 ? wrap_idx(z + dz - 1, nz) : 0);
-                    if (iv.x <= iv.y) {
-                        lo[dy][dz] = iv.x - s0;
-                        hi[dy][dz] = iv.y - s0;
-                    }
+            // the 3x3 neighbouring rows' intervals as nine named values (an
+            // array here could be placed in local memory)
+            auto nbr = [&](int dy, int dz) -> int2 {
+                if (D == 2 && dz != 0) return make_int2(1, 0);
+                const int2 iv = row_ivl(wrap_idx(y + dy, ny), D == 3 ? wrap_idx(z + dz, nz) : 0);
+                return iv.x <= iv.y ? make_int2(iv.x - s0, iv.y - s0) : make_int2(1, 0);
+            };
+            const int2 r00 = nbr(-1, -1), r10 = nbr(0, -1), r20 = nbr(1, -1);
+            const int2 r01 = nbr(-1, 0), r11 = nbr(0, 0), r21 = nbr(1, 0);
+            const int2 r02 = nbr(-1, 1), r12 = nbr(0, 1), r22 = nbr(1, 1);
+            auto iv_of = [&](int cy, int cz) -> int2 {  // cy, cz are constants after unrolling
+                switch ((cy + 1) * 3 + (cz + 1)) {
+                    case 0: return r00;
+                    case 1: return r01;
+                    case 2: return r02;
+                    case 3: return r10;
+                    case 4: return r11;
+                    case 5: return r12;
+                    case 6: return r20;
+                    case 7: return r21;
+                    default: return r22;
                 }
+            };
             int cl = ex, ch = -1;
 #pragma unroll
             for (int i = 1; i < L::Q; ++i) {
-                const int dy = L::cy(i) + 1, dz = L::cz(i) + 1;
-                if (lo[dy][dz] <= hi[dy][dz]) {
-                    cl = min(cl, lo[dy][dz] - L::cx(i));
-                    ch = max(ch, hi[dy][dz] - L::cx(i));
+                const int2 iv = iv_of(L::cy(i), L::cz(i));
+                if (iv.x <= iv.y) {
+                    cl = min(cl, iv.x - L::cx(i));
+                    ch = max(ch, iv.y - L::cx(i));
                 }
             }
             cl = max(cl, 0);
             ch = min(ch, ex - 1);
-            const int o0 = lo[1][1], o1 = hi[1][1];  // the row's own solid interval
+            const int o0 = r11.x, o1 = r11.y;  // the row's own solid interval
             int cnt = 0;
             for (int xr = cl; xr <= ch; ++xr) {
                 if (xr >= o0 && xr <= o1) {
@@ -479,9 +498,9 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
 #pragma unroll
                 for (int j = 1; j < L::Q; ++j) {
                     const int i = L::opp(j);  // source x - c_j = x + c_i
-                    const int dy = L::cy(i) + 1, dz = L::cz(i) + 1;
+                    const int2 iv = iv_of(L::cy(i), L::cz(i));
                     const int t = xr + L::cx(i);
-                    if (t >= lo[dy][dz] && t <= hi[dy][dz]) mask |= 1u << j;
+                    if (t >= iv.x && t <= iv.y) mask |= 1u << j;
                 }
                 if (!mask) continue;
                 if (out) out[cnt] = make_int2(wrap_idx(s0 + xr, nx) + nx * (y + ny * z), (int)mask);
