@@ -32,7 +32,10 @@ struct Graph {
     cudaGraphExec_t exec = nullptr;
 };
 
-constexpr int kGraphSteps = 16;
+constexpr int kGraphSteps = 16;  // ticks per CUDA graph of a batch
+// ticks per CUDA graph of one model: each graph ends by joining the side
+// stream (the last particle update), a bubble that longer graphs amortise
+constexpr int kModelGraphTicks = 64;
 
 }  // namespace
 
@@ -103,7 +106,7 @@ struct lbm_handle {
     // time
     long long tick = 0;
     double time = 0;
-    // graphs of kGraphSteps ticks: [profiling][starting buffer]
+    // graphs of kModelGraphTicks ticks: [profiling][starting buffer]
     Graph graphs[2][2];
     // profiling: per graph slot, events before/after the bulk kernel, after
     // the fix-up and after the particle kernel; plus the whole call
@@ -432,7 +435,7 @@ int prepare_tick(lbm_handle* h) {
 int launches_per_tick(const lbm_handle* h) {
     if (use_tick_kernel(h)) return 1;
     const bool fix = fixup_blocks(h) > 0;
-    return 1 + (fix ? 1 : 0) + (h->hparts.empty() ? 0 : 3);  // particles, links, links_sort
+    return 1 + (fix ? 1 : 0) + (h->hparts.empty() ? 0 : 1);  // the particle update rebuilds its links itself
 }
 
 // events of graph slot s: [0] before bulk, [1] after bulk, [2] after fix-up, [3] after particles
@@ -542,7 +545,7 @@ int build_graph(lbm_handle* h, int start) {
     cudaGraph_t graph = nullptr;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int b = start;
-    for (int s = 0; s < kGraphSteps; ++s) {
+    for (int s = 0; s < kModelGraphTicks; ++s) {
         enqueue_tick(h, b, s);
         b = 1 - b;
     }
@@ -1110,17 +1113,17 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_begin, h->stream));
     int64_t done = 0;
     int slots_used = 0;
-    while (nsteps - done >= kGraphSteps) {
+    while (nsteps - done >= kModelGraphTicks) {
         int rc = build_graph(h, h->cur);
         if (rc) return rc;
         CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling >= 2 ? 1 : 0][h->cur].exec, h->stream));
-        done += kGraphSteps;  // kGraphSteps is even: the buffer parity is unchanged
-        slots_used = kGraphSteps;
+        done += kModelGraphTicks;  // kModelGraphTicks is even: the buffer parity is unchanged
+        slots_used = kModelGraphTicks;
     }
     for (int s = 0; done < nsteps; ++done, ++s) {
-        enqueue_tick(h, h->cur, s % kGraphSteps);
+        enqueue_tick(h, h->cur, s % kModelGraphTicks);
         h->cur = 1 - h->cur;
-        slots_used = std::max(slots_used, std::min(s + 1, kGraphSteps));
+        slots_used = std::max(slots_used, std::min(s + 1, kModelGraphTicks));
     }
     join_particles(h);
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_end, h->stream));
@@ -1172,7 +1175,7 @@ int lbm_set_profiling(lbm_handle* h, int32_t on) {
     if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
     BIND(h);
     if (on && h->pev.empty()) {
-        h->pev.resize(4 * kGraphSteps);
+        h->pev.resize(4 * kModelGraphTicks);
         for (auto& e : h->pev) CUDA_TRY(h, cudaEventCreate(&e));
         CUDA_TRY(h, cudaEventCreate(&h->t_begin));
         CUDA_TRY(h, cudaEventCreate(&h->t_end));
