@@ -16,6 +16,7 @@ namespace lbm {
 
 constexpr int kIvlSmem = 512;  // rows of solid intervals staged in shared memory
 constexpr int kXSmem = 256;    // x coordinates of the solid box staged in shared memory
+constexpr int kLinkSmem = 2048;  // link entries staged in shared memory during a rebuild
 constexpr int kPartBlock = 256;  // CTA size of the stand-alone particle kernel
 
 struct ParticleArgs {
@@ -106,7 +107,85 @@ __device__ __forceinline__ void tile_bits_update(const ParticleArgs& a, const in
     }
 }
 
+// interval of row (y, z) of P's solid box (rows y-fastest from `rows`), or empty
+__device__ __forceinline__ int2 box_row_ivl(const ParticleDev& P, const int2* rows, int y, int z) {
+    if (y < P.slo[1] || y > P.shi[1] || z < P.slo[2] || z > P.shi[2]) return make_int2(1, 0);
+    return rows[(y - P.slo[1]) + (P.shi[1] - P.slo[1] + 1) * (z - P.slo[2])];
+}
+
+// The link entries of near-box row rr of P (near box ex x ey x .., x' = x - s0),
+// counted, and written to `out` unless it is null.  In x' coordinates every
+// row interval lies in [1, ex - 2] (the caller checks ex + 2 <= nx), so node
+// x' has a solid source x + c_i exactly when x' + c_i,x lies in the interval
+// of row (y + c_i,y, z + c_i,z); the candidates are the span of those shifted
+// intervals outside the row's own one.  A free function with its values in
+// registers: a lambda's captures or an indexed array could sit in local
+// memory, whose L1 lines the bulk pass running beside this kernel evicts.
 template <class L>
+__device__ __forceinline__ int near_row_links(const ParticleDev& P, const int2* rows, const GridDesc& g, int ex,
+                                              int ey, int s0, int rr, int2* out) {
+    constexpr int D = L::D;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const int y = wrap_idx(P.slo[1] - 1 + rr % ey, ny);
+    const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + rr / ey, nz) : 0;
+    auto nbr = [&](int dy, int dz) -> int2 {
+        if (D == 2 && dz != 0) return make_int2(1, 0);
+        const int2 iv = box_row_ivl(P, rows, wrap_idx(y + dy, ny), D == 3 ? wrap_idx(z + dz, nz) : 0);
+        return iv.x <= iv.y ? make_int2(iv.x - s0, iv.y - s0) : make_int2(1, 0);
+    };
+    const int2 r00 = nbr(-1, -1), r10 = nbr(0, -1), r20 = nbr(1, -1);
+    const int2 r01 = nbr(-1, 0), r11 = nbr(0, 0), r21 = nbr(1, 0);
+    const int2 r02 = nbr(-1, 1), r12 = nbr(0, 1), r22 = nbr(1, 1);
+    auto iv_of = [&](int cy, int cz) -> int2 {  // cy, cz are constants after unrolling
+        switch ((cy + 1) * 3 + (cz + 1)) {
+            case 0: return r00;
+            case 1: return r01;
+            case 2: return r02;
+            case 3: return r10;
+            case 4: return r11;
+            case 5: return r12;
+            case 6: return r20;
+            case 7: return r21;
+            default: return r22;
+        }
+    };
+    int cl = ex, ch = -1;
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        const int2 iv = iv_of(L::cy(i), L::cz(i));
+        if (iv.x <= iv.y) {
+            cl = min(cl, iv.x - L::cx(i));
+            ch = max(ch, iv.y - L::cx(i));
+        }
+    }
+    cl = max(cl, 0);
+    ch = min(ch, ex - 1);
+    const int o0 = r11.x, o1 = r11.y;  // the row's own solid interval
+    int cnt = 0;
+    for (int xr = cl; xr <= ch; ++xr) {
+        if (xr >= o0 && xr <= o1) {
+            xr = o1;
+            continue;
+        }
+        unsigned mask = 0;
+#pragma unroll
+        for (int j = 1; j < L::Q; ++j) {
+            const int i = L::opp(j);  // source x - c_j = x + c_i
+            const int2 iv = iv_of(L::cy(i), L::cz(i));
+            const int t = xr + L::cx(i);
+            if (t >= iv.x && t <= iv.y) mask |= 1u << j;
+        }
+        if (!mask) continue;
+        if (out) out[cnt] = make_int2(wrap_idx(s0 + xr, nx) + nx * (y + ny * z), (int)mask);
+        ++cnt;
+    }
+    return cnt;
+}
+
+// LK: link entries staged in shared memory during a rebuild (kLinkSmem for
+// the particle kernel; less inside the persistent tick kernel, whose CTAs
+// also hold the bulk and fix-up items' shared memory)
+template <class L, int LK = kLinkSmem>
 __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int p) {
     constexpr int D = L::D;
     const int tid = threadIdx.x;
@@ -117,6 +196,12 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
     __shared__ int s_warp[9];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
     __shared__ double s_xc[kXSmem];   // x coordinates of the solid box (interval rebuild)
+    // A rebuild's new intervals (s_ivl) and link entries (s_lk) are written to
+    // global memory at the end, coalesced: scattered stores issued in between
+    // drain slowly beside the bulk pass and hold up the shared-memory accesses
+    // queued behind them.
+    __shared__ int2 s_lk[LK];
+    __shared__ int s_lkn;  // entries [0, s_lkn) of the new list are in s_lk
     // the particle record is staged in shared memory: the update below is a
     // serial chain of reads and writes that must not go to global memory
     __shared__ ParticleDev sP;
@@ -332,7 +417,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             // non-negative doubles order like their bit patterns
             atomicMin(&s_slack, (unsigned long long)__double_as_longlong(slack));
             if (old.x != xlo || old.y != xhi) changed = 1;
-            *slot = make_int2(xlo, xhi);
+            if (s_rows > kIvlSmem) *slot = make_int2(xlo, xhi);  // else written at the end
             if (r < kIvlSmem) s_ivl[r] = make_int2(xlo, xhi);
             if (xlo <= xhi) s_nonempty = 1;
         }
@@ -441,74 +526,17 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             }
             return cnt;
         };
-        // Fast form (the near box narrower than the x axis by two): in x' = x - s0
-        // coordinates every row interval lies in [1, ex - 2], so node x' of a row
-        // has a solid source x + c_i exactly when x' + c_i,x lies in the
-        // interval of row (y + c_i,y, z + c_i,z); the candidates are the span
-        // of those shifted intervals outside the row's own one.  Everything is
-        // held in registers (an indexed local array would sit in L1, which the
-        // bulk pass running beside this kernel evicts).
+        // fast form (near_row_links) where the near box is narrower than the x
+        // axis by two; the node-by-node scan above otherwise
         const int s0 = P.slo[0] - 1;
         const bool fast = ex + 2 <= nx;
+        const int2* ivl_rows = ivl_smem ? s_ivl : a.ivl + P.ivl_off;
         auto row_links = [&](int rr, int2* out) -> int {
-            const int y = wrap_idx(P.slo[1] - 1 + rr % ey, ny);
-            const int z = D == 3 ? wrap_idx(P.slo[2] - 1 + rr / ey, nz) : 0;
-            // the 3x3 neighbouring rows' intervals as nine named values (an
-            // array here could be placed in local memory)
-            auto nbr = [&](int dy, int dz) -> int2 {
-                if (D == 2 && dz != 0) return make_int2(1, 0);
-                const int2 iv = row_ivl(wrap_idx(y + dy, ny), D == 3 ? wrap_idx(z + dz, nz) : 0);
-                return iv.x <= iv.y ? make_int2(iv.x - s0, iv.y - s0) : make_int2(1, 0);
-            };
-            const int2 r00 = nbr(-1, -1), r10 = nbr(0, -1), r20 = nbr(1, -1);
-            const int2 r01 = nbr(-1, 0), r11 = nbr(0, 0), r21 = nbr(1, 0);
-            const int2 r02 = nbr(-1, 1), r12 = nbr(0, 1), r22 = nbr(1, 1);
-            auto iv_of = [&](int cy, int cz) -> int2 {  // cy, cz are constants after unrolling
-                switch ((cy + 1) * 3 + (cz + 1)) {
-                    case 0: return r00;
-                    case 1: return r01;
-                    case 2: return r02;
-                    case 3: return r10;
-                    case 4: return r11;
-                    case 5: return r12;
-                    case 6: return r20;
-                    case 7: return r21;
-                    default: return r22;
-                }
-            };
-            int cl = ex, ch = -1;
-#pragma unroll
-            for (int i = 1; i < L::Q; ++i) {
-                const int2 iv = iv_of(L::cy(i), L::cz(i));
-                if (iv.x <= iv.y) {
-                    cl = min(cl, iv.x - L::cx(i));
-                    ch = max(ch, iv.y - L::cx(i));
-                }
-            }
-            cl = max(cl, 0);
-            ch = min(ch, ex - 1);
-            const int o0 = r11.x, o1 = r11.y;  // the row's own solid interval
-            int cnt = 0;
-            for (int xr = cl; xr <= ch; ++xr) {
-                if (xr >= o0 && xr <= o1) {
-                    xr = o1;
-                    continue;
-                }
-                unsigned mask = 0;
-#pragma unroll
-                for (int j = 1; j < L::Q; ++j) {
-                    const int i = L::opp(j);  // source x - c_j = x + c_i
-                    const int2 iv = iv_of(L::cy(i), L::cz(i));
-                    const int t = xr + L::cx(i);
-                    if (t >= iv.x && t <= iv.y) mask |= 1u << j;
-                }
-                if (!mask) continue;
-                if (out) out[cnt] = make_int2(wrap_idx(s0 + xr, nx) + nx * (y + ny * z), (int)mask);
-                ++cnt;
-            }
-            return cnt;
+            return near_row_links<L>(P, ivl_rows, a.g, ex, ey, s0, rr, out);
         };
         int base = 0;
+        if (tid == 0) s_lkn = LK;
+        __syncthreads();
         for (int r0 = 0; r0 < nrows; r0 += blockDim.x) {
             const int rr = r0 + tid;
             const int c = rr < nrows ? (fast ? row_links(rr, nullptr) : scan_row(rr, nullptr)) : 0;
@@ -534,15 +562,21 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             const int off = base + s_warp[warp] + v - c;
             if (c > 0) {
                 if (off + c <= P.link_cap) {
-                    if (fast) row_links(rr, a.links + P.link_off + off);
-                    else scan_row(rr, a.links + P.link_off + off);
+                    // rows that fit go to shared memory; they form a prefix of the list
+                    int2* out = off + c <= LK ? s_lk + off : a.links + P.link_off + off;
+                    if (off + c > LK) atomicMin(&s_lkn, off);
+                    if (fast) row_links(rr, out);
+                    else scan_row(rr, out);
                 }
                 else atomicOr(a.err, kErrLinkOverflow);
             }
             base += s_warp[8];
             __syncthreads();
         }
-        if (tid == 0) P.nlinks = base < P.link_cap ? base : P.link_cap;
+        if (tid == 0) {
+            P.nlinks = base < P.link_cap ? base : P.link_cap;
+            s_lkn = min(s_lkn, (int)P.nlinks);
+        }
     }
     __syncthreads();
 
@@ -555,6 +589,11 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
         if (s_newbox[3] * s_newbox[4] * s_newbox[5] > 0) tile_bits_update(a, s_newbox, s_newbox + 3, p, true);
     }
     __syncthreads();
+    // the staged intervals and link entries, coalesced
+    if (s_changed && s_rows <= kIvlSmem)
+        for (int r = tid; r < s_rows; r += blockDim.x) a.ivl[P.ivl_off + r] = s_ivl[r];
+    if (s_changed && a.inline_links)
+        for (int e = tid; e < s_lkn; e += blockDim.x) a.links[P.link_off + e] = s_lk[e];
     {
         const unsigned long long* ssrc = reinterpret_cast<const unsigned long long*>(&sP);
         unsigned long long* gdst = reinterpret_cast<unsigned long long*>(a.parts + p);

@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
         } else if (t < nabc) {
             cta_wait(&q->cnt_b, (int)it.nb, err);
             const int2 m = it.cmap[t - nab];
-            particles_body<L>(pargs[m.x], m.y);
+            particles_body<L, 128>(pargs[m.x], m.y);
         } else {
             const int2 m = it.dmap[t - nabc];
             const StepArgs& A = args[m.x];
