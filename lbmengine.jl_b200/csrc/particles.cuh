@@ -17,7 +17,9 @@ namespace lbm {
 constexpr int kIvlSmem = 512;  // rows of solid intervals staged in shared memory
 constexpr int kXSmem = 256;    // x coordinates of the solid box staged in shared memory
 constexpr int kLinkSmem = 2048;  // link entries staged in shared memory during a rebuild
-constexpr int kPartBlock = 256;  // CTA size of the stand-alone particle kernel
+constexpr int kPartBlock = 512;  // CTA size of the stand-alone particle kernel (one near-box row
+                                 // per thread in a link rebuild of a particle up to r ~ 10)
+constexpr int kMaxPartWarps = 32;
 
 struct ParticleArgs {
     ParticleDev* parts;
@@ -189,11 +191,11 @@ template <class L, int LK = kLinkSmem>
 __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int p) {
     constexpr int D = L::D;
     const int tid = threadIdx.x;
-    __shared__ double s_red[8][6];
+    __shared__ double s_red[kMaxPartWarps][6];
     __shared__ int s_moved, s_oldbox[6], s_newbox[6], s_changed, s_rows, s_bad, s_nonempty, s_keep;
     __shared__ unsigned long long s_slack;  // bit pattern of a non-negative double
     __shared__ unsigned s_links;
-    __shared__ int s_warp[9];
+    __shared__ int s_warp[kMaxPartWarps + 1];
     __shared__ int2 s_ivl[kIvlSmem];  // the particle's solid intervals during a link rebuild
     __shared__ double s_xc[kXSmem];   // x coordinates of the solid box (interval rebuild)
     // A rebuild's new intervals (s_ivl) and link entries (s_lk) are written to
@@ -556,7 +558,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
                     s_warp[w] = run;
                     run += t;
                 }
-                s_warp[8] = run;
+                s_warp[kMaxPartWarps] = run;
             }
             __syncthreads();
             const int off = base + s_warp[warp] + v - c;
@@ -570,7 +572,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
                 }
                 else atomicOr(a.err, kErrLinkOverflow);
             }
-            base += s_warp[8];
+            base += s_warp[kMaxPartWarps];
             __syncthreads();
         }
         if (tid == 0) {
