@@ -569,13 +569,16 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
 
 // Resident threads per SM the vector bulk kernels are compiled for: a D2Q9
 // thread holds 36 populations and fits 64 registers (32 warps per SM); the
-// 3D sets take up to 128 (16 warps per SM).
-template <class L>
-constexpr int bulk_threads_per_sm() { return L::Q <= 9 ? 1024 : 512; }
+// 3D sets take up to 128 (16 warps per SM) with FP32/FP64 storage, which is
+// memory-bound, and up to 96 (20 warps per SM) with 2-byte storage, whose
+// conversions make it issue-bound as well: the extra warps took its 128^3
+// pass from 28.4 to 26.9 us, with no change for FP32.
+template <class L, int ST = ST_F32>
+constexpr int bulk_threads_per_sm() { return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? 640 : 512); }
 
 // the vector bulk pass over all tiles, one CTA of B threads per tile
 template <class L, int ST, bool TRT, int B>
-__global__ void __launch_bounds__(B, bulk_threads_per_sm<L>() / B) k_bulk_v4(const StepArgs a) {
+__global__ void __launch_bounds__(B, bulk_threads_per_sm<L, ST>() / B) k_bulk_v4(const StepArgs a) {
     __shared__ float s_ex[x_moving_dirs<L>()][B];
     grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
     bulk_v4_tile<L, ST, TRT, B>(a, blockIdx.x, s_ex);

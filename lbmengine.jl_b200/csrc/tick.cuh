@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
 // The bulk tiles of a batch, one CTA per item of the D map (no queue): the
 // replicas' arguments come from `args[dmap[i].x]`.
 template <class L, int ST, bool TRT>
-__global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L>() / kTickBlock)
+__global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L, ST>() / kTickBlock)
     k_bulk_batch(const StepArgs* __restrict__ args, const int2* __restrict__ dmap) {
     __shared__ float s_ex[x_moving_dirs<L>()][kTickBlock];
     const int2 m = dmap[blockIdx.x];
