@@ -74,7 +74,7 @@ __device__ __forceinline__ void ladd_link(const StepArgs& a, const ParticleDev& 
 // grid_dep_wait(): launched with a programmatic edge from the bulk pass, the
 // kernel computes during the bulk pass's last wave.
 template <class L, int ST, bool TRT, int NT>
-__device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b) {
+__device__ __forceinline__ bool fixup_body(const StepArgs& a, const long long b) {
     static_assert(NT >= kFixBlock && NT % 32 == 0 && kFixBlock == 64, "fix-up CTA shape");
     using SS = Store<ST>;
     using T = typename SS::T;
@@ -107,7 +107,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         const T z0 = SS::enc(R(-a.rho0), R(a.scale));
         grid_dep_wait();
         for (int s = tid; s < n * Q; s += NT) dst[(long long)(s % Q) * N + a.wnodes[k0 + s / Q]] = z0;
-        return;
+        return true;
     }
     const bool is_part = b < npb;
     int p = -1, chunk = 0;
@@ -127,7 +127,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         }
         if (tid < kFixBlock && e < lcap) ent = a.links[loff + e];  // in the list's capacity
         const int nl = a.parts[p].nlinks;
-        if (chunk * kFixBlock >= nl) return;  // uniform: chunk past the link list
+        if (chunk * kFixBlock >= nl) return false;  // uniform: chunk past the link list
         valid = tid < kFixBlock && e < nl;
         const unsigned long long* gsrc = reinterpret_cast<const unsigned long long*>(a.parts + p);
         unsigned long long* sdst = reinterpret_cast<unsigned long long*>(&sP);
@@ -281,7 +281,7 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         const int item = s_list[l];
         dst[(item & 31) * N + s_cell[item >> 5]] = SS::enc(s_val[l], R(a.scale));
     }
-    if (!is_part) return;
+    if (!is_part) return true;
     // fixed-order reduction: butterfly inside warps, warps summed in order
 #pragma unroll
     for (int k = 0; k < 6; ++k)
@@ -294,11 +294,49 @@ __device__ __forceinline__ void fixup_body(const StepArgs& a, const long long b)
         for (int w = 0; w < NT / 32; ++w) sum += s_red[w][tid];
         a.partial[(long long)(sP.part_off + chunk) * kPartialStride + tid] = sum;
     }
+    return true;
 }
 
 template <class L, int ST, bool TRT>
 __global__ void __launch_bounds__(kFixThreads) k_fixup(const StepArgs a) {
     fixup_body<L, ST, TRT, kFixThreads>(a, blockIdx.x);
+}
+
+// Many particles: k_fixup_walk.  Its CTA g of a particle walks chunks g,
+// g + G, ... of the particle's list up to the list's end, so the CTAs past the
+// lists' ends number G - chunks per particle rather than the capacity's
+// chunks (the capacity is the near box; 64 particles of r = 6 in 192^3 launch
+// 2,048 CTAs instead of 8,000).  With one particle k_fixup is faster: the
+// walk costs registers, and the CTAs past the list end overlap the others.
+constexpr int kFixCtasPerPart = 32;
+constexpr long long kFixWalkMin = 1024;  // particle CTAs of k_fixup from which k_fixup_walk is used
+__host__ __device__ __forceinline__ int fixup_ctas_per_particle(int maxchunks) {
+    return maxchunks < kFixCtasPerPart ? maxchunks : kFixCtasPerPart;
+}
+
+// one chunk, as a called function (the parameter block is addressed in place)
+template <class L, int ST, bool TRT>
+__device__ __noinline__ bool fixup_chunk(const StepArgs& a, const long long b) {
+    return fixup_body<L, ST, TRT, kFixThreads>(a, b);
+}
+
+// Grid: nparts * fixup_ctas_per_particle(maxchunks) CTAs, chunk-major (the
+// first chunks of every particle first), then one per wall-link or
+// wall-node block.
+template <class L, int ST, bool TRT>
+__global__ void __launch_bounds__(kFixThreads, 2) k_fixup_walk(const __grid_constant__ StepArgs a) {
+    const long long bi = blockIdx.x;
+    const int G = fixup_ctas_per_particle(a.maxchunks);
+    const long long pb = (long long)a.nparts * G;
+    if (bi >= pb) {
+        fixup_chunk<L, ST, TRT>(a, (long long)a.nparts * a.maxchunks + (bi - pb));
+        return;
+    }
+    const int p = (int)(bi % a.nparts);
+    for (int c = (int)(bi / a.nparts); c < a.maxchunks; c += G) {
+        if (!fixup_chunk<L, ST, TRT>(a, (long long)p * a.maxchunks + c)) break;
+        __syncthreads();  // shared memory is reused by the next chunk
+    }
 }
 
 }  // namespace lbm

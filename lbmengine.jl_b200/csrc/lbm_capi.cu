@@ -364,6 +364,17 @@ long long fixup_blocks(const lbm_handle* h) {
            (h->nwnodes + kFixBlock - 1) / kFixBlock;
 }
 
+// the fix-up walks the lists' chunks (k_fixup_walk) when a CTA per chunk of
+// every list's capacity would be many CTAs
+bool fixup_walk(const lbm_handle* h) { return (long long)h->hparts.size() * h->maxchunks >= kFixWalkMin; }
+
+// CTAs of a fix-up launch
+long long fixup_grid(const lbm_handle* h) {
+    if (!fixup_walk(h)) return fixup_blocks(h);
+    return (long long)h->hparts.size() * fixup_ctas_per_particle(h->maxchunks) +
+           (h->nwlinks + kFixBlock - 1) / kFixBlock + (h->nwnodes + kFixBlock - 1) / kFixBlock;
+}
+
 // the persistent tick kernel applies to the vector bulk kernel with
 // kTickBlock-thread tiles, when there is boundary work to overlap
 bool use_tick_kernel(const lbm_handle* h) {
@@ -515,7 +526,7 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
     const long long nb = fixup_blocks(h);
     if (nb > 0) {
         if (bulk_node) programmatic_from(h->stream, bulk_node);
-        h->ops.fixup(a, (unsigned)nb, h->stream, early && !bulk_node && !waited);
+        h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, early && !bulk_node && !waited, fixup_walk(h));
     }
     if (a.nparts == 0) prof_record(h, slot, 2, h->stream);
     if (a.nparts > 0) {
@@ -1230,7 +1241,7 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
             launch_bulk(h, a, h->stream);
             b = 1 - b;
         } else if (kernel == LBM_KERNEL_FIXUP) {
-            h->ops.fixup(a, (unsigned)fixup_blocks(h), h->stream, false);
+            h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, false, fixup_walk(h));
         } else if (kernel == LBM_KERNEL_TICK) {
             h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
             b = 1 - b;
@@ -1657,7 +1668,7 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
         const StepArgs a = noalloc_step_args(h, h->cur, scratch);
         pa.nbox_out[0] = h->d_nbox[h->cur];
         launch_bulk(h, a, h->stream);
-        if (nb > 0) h->ops.fixup(a, (unsigned)nb, h->stream, false);
+        if (nb > 0) h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, false, fixup_walk(h));
         if (np > 0) {
             h->ops.particles(pa, (unsigned)np, h->stream);
             h->ops.links(pa, np, h->link_bpp, h->d_linkcnt, h->stream);

@@ -14,7 +14,8 @@ struct Ops {
     void (*bulk)(const StepArgs&, unsigned grid, dim3 block, cudaStream_t);
     // early: launch with programmatic stream serialization (the fix-up may
     // start while the kernel before it in the stream still runs)
-    void (*fixup)(const StepArgs&, unsigned grid, cudaStream_t, bool early);
+    // walk: the chunk-walking kernel (k_fixup_walk), whose grid is fixup_walk_grid
+    void (*fixup)(const StepArgs&, unsigned grid, cudaStream_t, bool early, bool walk);
     void (*particles)(const ParticleArgs&, unsigned grid, cudaStream_t);
     // link-list rebuild of flagged particles: two passes of blocks_per_particle
     // CTAs per particle; counts holds nparts * blocks_per_particle ints
@@ -49,7 +50,7 @@ struct OpsImpl {
     static void bulk(const StepArgs& a, unsigned grid, dim3 block, cudaStream_t s) {
         k_bulk<L, ST, TRT><<<grid, block, 0, s>>>(a);
     }
-    static void fixup(const StepArgs& a, unsigned grid, cudaStream_t s, bool early) {
+    static void fixup(const StepArgs& a, unsigned grid, cudaStream_t s, bool early, bool walk) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(grid);
         cfg.blockDim = dim3(kFixThreads);
@@ -59,7 +60,8 @@ struct OpsImpl {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = early ? 1 : 0;
-        cudaLaunchKernelEx(&cfg, k_fixup<L, ST, TRT>, a);
+        if (walk) cudaLaunchKernelEx(&cfg, k_fixup_walk<L, ST, TRT>, a);
+        else cudaLaunchKernelEx(&cfg, k_fixup<L, ST, TRT>, a);
     }
     static void particles(const ParticleArgs& a, unsigned grid, cudaStream_t s) {
         k_particles<L><<<grid, kPartBlock, 0, s>>>(a);

@@ -90,6 +90,17 @@ CASES = {
                         coupleForces=True, coupleTorques=True, swimmingDirection=seeded_direction(9, 3),
                         massDensity=3.0)],
         steps=30),
+    # twelve squirmers: more fix-up CTAs than the one-chunk-per-CTA launch
+    # takes (nparts x capacity chunks >= 1024), so the chunk-walking fix-up runs
+    "d3q19_twelve_squirmers": dict(
+        model=dict(dims=3, velocities="D3Q19", collisionModel="trt", latticeParameter=1.0,
+                   relaxationTimeRatio=0.8, xlims=(-24.0, 23.0), ylims=(-16.0, 15.0), zlims=(-16.0, 15.0)),
+        particles=[dict(kind="squirmer", radius=5.0, position=[-16.0 + 16.0 * i + 0.3, -8.0 + 16.0 * j - 0.2,
+                                                                -8.0 + 16.0 * k + 0.1],
+                        swimmingSpeed=1e-3, beta=float(2 * i - j - k), coupleForces=True, coupleTorques=True,
+                        swimmingDirection=seeded_direction(20 + 4 * i + 2 * j + k, 3), massDensity=3.0)
+                   for i in range(3) for j in range(2) for k in range(2)],
+        steps=30),
     "d2q9_incompressible": dict(
         model=dict(dims=2, latticeParameter=1.0, relaxationTimeRatio=0.8, collisionModel="trt",
                    xlims=(-16.0, 15.0), isFluidCompressible=False, massDensity=1.0,
