@@ -456,7 +456,9 @@ template <> struct Vec4<ST_F32> {
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     }
     static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
-        *reinterpret_cast<float4*>(static_cast<float*>(base) + cell0) = make_float4(a0, a1, a2, a3);
+        // streaming (evict-first) store: the next read of the line is a tick away,
+        // after the pass has streamed far more than L2 through the cache
+        __stcs(reinterpret_cast<float4*>(static_cast<float*>(base) + cell0), make_float4(a0, a1, a2, a3));
     }
 };
 template <> struct Vec4<ST_F16> {
@@ -472,7 +474,7 @@ template <> struct Vec4<ST_F16> {
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
-        *reinterpret_cast<uint2*>(static_cast<__half*>(base) + cell0) = q;
+        __stcs(reinterpret_cast<uint2*>(static_cast<__half*>(base) + cell0), q);  // streaming, as above
     }
 };
 template <> struct Vec4<ST_BF16> {
@@ -488,7 +490,7 @@ template <> struct Vec4<ST_BF16> {
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
-        *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(base) + cell0) = q;
+        __stcs(reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(base) + cell0), q);  // streaming, as above
     }
 };
 
