@@ -54,9 +54,16 @@ def workload(side=128, storage="f32", device=-1):
     return model, squirmer
 
 
-def workload_name(side, storage):
-    return (f"D3Q19 TRT(3/16) {side}^3 periodic, tau=0.7, Guo F=1e-6 x, 1 squirmer r=8 B1=5e-4 beta=+5, "
-            f"{storage} shifted storage")
+def workload_name(side, storage=None):
+    name = f"D3Q19 TRT(3/16) {side}^3 periodic, tau=0.7, Guo F=1e-6 x, 1 squirmer r=8 B1=5e-4 beta=+5"
+    return name if storage is None else f"{name}, {storage} shifted storage"
+
+
+def bench_config(side, world):
+    """The `config` object of the JSON line; both arms print the same one."""
+    return {"workload": workload_name(side), "cells": side ** 3,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": f"inputs larger than L2: D3Q19 populations 2 x {side ** 3 * 19 * 4 / 1e6:.0f} MB (FP32)"}
 
 
 def measured_peak():
@@ -69,7 +76,8 @@ def measured_peak():
 
 
 def bulk_traffic(storage, cells):
-    """DRAM bytes per bulk launch from the ncu capture summarised in profiles/bulk_traffic.txt."""
+    """DRAM bytes per bulk launch, replayed from an earlier ncu capture of the same kernel
+    (bytes per cell, profiles/bulk_traffic.txt) scaled to `cells`: not measured by this run."""
     path = os.path.join(REPO, "profiles", "bulk_traffic.txt")
     try:
         for line in open(path):
@@ -170,6 +178,12 @@ def barrier(dist):
         dist.barrier()
 
 
+ORACLE_SEMANTICS = ("FP64 C++ restatement of the reference's tick (fluid step of src/gpu/fluids.jl:132-226 "
+                    "with the GPU module's particle update, the path this library replaces; the CPU module's "
+                    "particle rules are a switch of the same code), OpenMP over cells; the reference itself is "
+                    "Julia and cannot run here")
+
+
 def oracle_mlups(side, ticks, warm, threads=None):
     """FP64 CPU oracle on a side^3 box of the workload: (MLUPS, seconds, threads)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -201,17 +215,16 @@ def run_reference(args):
     world, rank, _, _ = dist_setup_env_only()
     if rank != 0:
         return 0
-    side = oracle_side_for(args.steps + args.warmup, budget_s=150.0)
+    side = args.side
     mlups, dt, threads = oracle_mlups(side, args.steps, args.warmup)
     line = {
         "metric": METRIC, "impl": "reference", "value": round(mlups, 4), "unit": "MLUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(128, "f64"), "parallelism": "replicas"},
+        "config": bench_config(side, world),
         "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": threads, "kind": "port",
-                         "sample": f"{side}^3 box of the workload (same physics, one squirmer), {args.steps} ticks "
-                                   f"after {args.warmup} warm-up ticks; FP64 C++ restatement of the reference's "
-                                   f"GPU-module tick (Julia reference not runnable here)"},
+                         "sample": f"the full {side}^3 workload, {args.steps} ticks after {args.warmup} warm-up "
+                                   f"ticks on this host's cores; {ORACLE_SEMANTICS}"},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -266,6 +279,7 @@ def run_ours(args):
                 "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
                 "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
+                "traffic_source": "replayed from an earlier ncu capture (profiles/bulk_traffic.txt), not this run",
                 "kernel": f"k_bulk_v4<D3Q19,{storage},TRT,64>", "bytes_per_launch": bulk_bytes,
                 "algorithmic_bytes_per_cell": 2 * q * bpp, "kernel_ms": kern,
                 "fixup_entries": prof.fixup_entries,
@@ -307,8 +321,8 @@ def run_ours(args):
         ticks = args.cpu_ticks
         mlups, dt, threads = oracle_mlups(side, ticks, 1)
         cpu = {"value": round(mlups, 4), "unit": "MLUPS", "cores": threads, "kind": "port",
-               "sample": f"{ticks} ticks (after 1 warm-up tick) of the full {side}^3 workload, FP64 C++ restatement "
-                         f"of the reference's GPU-module tick, OpenMP over cells ({dt:.1f} s)"}
+               "sample": f"{ticks} ticks (after 1 warm-up tick) of the full {side}^3 workload ({dt:.1f} s); "
+                         f"{ORACLE_SEMANTICS}"}
     clocks = clk.summary()
     forms = run_forms(args, local) if rank == 0 and world == 1 else None
     if rank == 0:
@@ -317,14 +331,14 @@ def run_ours(args):
             "warmup": max(3, args.warmup), "ms_per_step": round(tick_ms, 6), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if storage == "f64" else "f32",
             "data": "synthetic",
-            "config": {"workload": workload_name(side, storage), "cells": cells, "storage": storage,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": f"inputs larger than L2: populations 2 x {cells * q * bpp / 1e6:.0f} MB"},
+            "config": bench_config(side, world), "storage": storage,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                        "samples": clocks["samples"]},
             "forms": forms,
         }
+        if forms:
+            line["forms_summary"] = forms_summary(forms)  # last key: survives a tail of the output
         print(json.dumps(line), flush=True)
     m.close()
     if dist is not None:
@@ -418,9 +432,14 @@ def form_precision_c3(device, ticks=3000, density=3.0):
     m = M.LBMmodel(config.resolve_model(**dict(model, storage="f64")))
     for p in parts:
         M._add(m, config.resolve_squirmer(3, **p))
+    from lbmengine._capi import LbmError
     diverged = None
     for _ in range(20):
-        m.step(100)
+        try:
+            m.step(100)  # the density sentinel raises once the run has diverged
+        except LbmError:
+            diverged = m.tick
+            break
         if not np.isfinite(m.fluidVelocity).all():
             diverged = m.tick
             break
@@ -481,6 +500,7 @@ def form_batch(device, ticks=2000, sampled=8):
            "tuning": vars(chosen), "candidates": len(cands),
            "hbm_frac_of_measured": round(b.cells * 72 / (ms / 1e3) / 1e9 / measured_peak()[0], 4),
            "replicas_nonfinite_at_end": len(nonfinite),
+           "replicas_diverged": sum(1 for st in b.status() if st != 0),
            "note": "replicas with low tau and a large radius diverge under the reference's explicit Ladd coupling at "
                    "particle density 1 (the FP64 oracle diverges on them too); they cost the same per tick"}
     # the same replicas one at a time (each model's own graph-replayed tick)
@@ -604,12 +624,153 @@ def form_gradients(device, ticks=3000, window=(1000, 3000), dual_side=32, dual_t
     return out
 
 
+def _oracle_errors(res, gpu, orc):
+    """Errors of a GPU model against an oracle model: rel. L2 of rho and u, the
+    largest position error (lattice units), the force error relative to the
+    oracle's largest component."""
+    import numpy as np
+    rho_o, u_o = orc.fields()
+    d = res.dims
+    rho_g = gpu.massDensity.ravel(order="F")
+    u_g = gpu.fluidVelocity.reshape(-1, d, order="F").T
+    a, b = gpu.particle_states()[0], orc.particles()[0]
+    fo = np.array(b.last_force[:d])
+    return {"rho_rel_l2": _rel_l2(rho_g, rho_o), "u_rel_l2": _rel_l2(u_g, u_o),
+            "position_abs_err": float(np.max(np.abs(np.array(a.position[:d]) - np.array(b.position[:d])))),
+            "force_rel_err": float(np.max(np.abs(np.array(a.last_force[:d]) - fo)) / max(1e-30, np.max(np.abs(fo))))}
+
+
+def form_parity(device, c2_ticks=500, c1_ticks=5000):
+    """The plain-method workloads against the FP64 CPU oracle at full size:
+    the 128^3 D3Q19 TRT squirmer box for beta in {-5, 0, +5} over c2_ticks
+    ticks (FP32, FP16, BF16 storage against one oracle run per beta), and the
+    256 x 128 D2Q9 BGK squirmer over c1_ticks ticks (centred coordinates; as
+    specified, with the squirmer 4x too light by the reference's origin-centred
+    mass, both the oracle and the GPU diverge, and the tick of the GPU's
+    divergence report is given)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the checker
+    from lbmengine import _capi, config, model as M
+    oracle.build()
+    out = {"c2": {"config": workload_name(128) + f" with beta in (-5, 0, +5); {c2_ticks} ticks; oracle FP64"}}
+    for beta in (-5.0, 0.0, 5.0):
+        mkw, skw = workload(128, "f64", device=device)
+        skw = dict(skw, beta=beta)
+        t0 = time.perf_counter()
+        orc = oracle.OracleModel(config.resolve_model(**mkw))
+        orc.add_particle(config.resolve_squirmer(3, **skw))
+        orc.step(c2_ticks)
+        ent = {"oracle_s": round(time.perf_counter() - t0, 1)}
+        for st in ("f32", "f16", "bf16"):
+            mkw2, _ = workload(128, st, device=device)
+            res = config.resolve_model(**mkw2)
+            g = M.LBMmodel(res)
+            M._add(g, config.resolve_squirmer(3, **skw))
+            g.step(c2_ticks)
+            ent[st] = _oracle_errors(res, g, orc)
+            g.close()
+        orc.close()
+        out["c2"][f"beta={beta:+g}"] = ent
+    # C1
+    out["c1"] = {"config": f"D2Q9 BGK 256x128, tau=0.8, squirmer r=10 B1=1e-3 beta=+3, angle 0; {c1_ticks} ticks"}
+    for centred in (True, False):
+        lims = dict(xlims=(-128.0, 127.0), ylims=(-64.0, 63.0)) if centred else dict(xlims=(0.0, 255.0),
+                                                                                  ylims=(0.0, 127.0))
+        pos = [-64.0, 0.0] if centred else [64.0, 64.0]
+        prm = config.resolve_squirmer(2, radius=10, position=pos, swimmingDirection=[1.0, 0.0],
+                                      swimmingSpeed=1e-3 / 1.5, beta=3.0, coupleForces=True, coupleTorques=True)
+        key = "centred" if centred else "as_specified"
+        ent = {}
+        for st in ("f64", "f32"):
+            res = config.resolve_model(dims=2, latticeParameter=1.0, relaxationTimeRatio=0.8, collisionModel="bgk",
+                                       storage=st, device=device, **lims)
+            orc = oracle.OracleModel(res)
+            orc.add_particle(prm)
+            g = M.LBMmodel(res)
+            M._add(g, prm)
+            if centred:
+                orc.step(c1_ticks)
+                g.step(c1_ticks)
+                ent[st] = _oracle_errors(res, g, orc)
+            else:
+                orc.step(1000)
+                g.step(1000)
+                ent[st] = {"at_tick_1000": _oracle_errors(res, g, orc)}
+                reported = None
+                while g.tick < c1_ticks:
+                    try:
+                        g.step(250)
+                    except _capi.LbmError as exc:
+                        reported = (g.tick, exc.code)
+                        break
+                orc.step(c1_ticks - 1000)
+                ent[st]["gpu_divergence_reported_at_tick"] = reported[0] if reported else None
+                ent[st]["oracle_finite_at_end"] = bool(np.isfinite(orc.fields()[1]).all())
+            g.close()
+            orc.close()
+        out["c1"][key] = ent
+    return out
+
+
+def _r(x, n=3):
+    return None if x is None else float(f"{x:.{n}g}")
+
+
+def forms_summary(forms):
+    """One compact entry per form (throughput ratios and the largest errors)."""
+    out = {}
+    f = forms.get("precision_c2", {})
+    if "f32" in f:
+        out["precision_c2"] = {"mlups": {k: f[k]["mlups"] for k in ("f32", "f16", "bf16")},
+                               "f16_vs_f32": f.get("f16_vs_f32"), "bf16_vs_f32": f.get("bf16_vs_f32"),
+                               "u_err_vs_f64": {k: _r(f[k]["u_rel_l2"]) for k in ("f32", "f16", "bf16")}}
+    f = forms.get("precision_c3", {})
+    if "f32" in f:
+        out["precision_c3"] = {"mlups": {k: f[k]["mlups"] for k in ("f32", "f16", "bf16")},
+                               "f16_vs_f32": round(f["f16"]["mlups"] / f["f32"]["mlups"], 3),
+                               "u_err_vs_f64": {k: _r(f[k]["u_rel_l2"]) for k in ("f32", "f16", "bf16")}}
+    f = forms.get("batching_c4", {})
+    if "mlups" in f:
+        chk = [e for e in f.get("oracle_check", []) if e["oracle_finite"]]
+        out["batching_c4"] = {"mlups": f["mlups"], "hbm_frac": f["hbm_frac_of_measured"],
+                              "vs_one_at_a_time": f["batch_vs_one_at_a_time"],
+                              "diverged_replicas": f.get("replicas_diverged"),
+                              "oracle_u_err_max": _r(max((e["u_rel_l2"] for e in chk), default=None))}
+    f = forms.get("gradients_c5", {})
+    if "f32" in f:
+        cd = f.get("central_differences", {})
+        out["gradients_c5"] = {"s": round(f["f32"]["ms"] / 1e3, 1),
+                               "dual_rel_err_max": _r(max(f["dual_check"]["rel_err"].values())),
+                               "fd_rel_err_max": {h: _r(max(v["rel_err_f64_adjoint"] for v in cd[h].values()))
+                                                  for h in cd}}
+        if "drag" in f:
+            out["gradients_c5"]["drag_fd_rel_err_max"] = f["drag"].get("fd_rel_err_max")
+    f = forms.get("parity", {})
+    if "c2" in f:
+        out["parity_c2_500"] = {b: {st: {"u": _r(v[st]["u_rel_l2"], 2), "rho": _r(v[st]["rho_rel_l2"], 2),
+                                         "pos": _r(v[st]["position_abs_err"], 2)} for st in ("f32", "f16", "bf16")}
+                                for b, v in f["c2"].items() if b.startswith("beta")}
+        c1 = f["c1"]
+        out["parity_c1_5000"] = {"centred": {st: {"u": _r(c1["centred"][st]["u_rel_l2"], 2),
+                                                  "pos": _r(c1["centred"][st]["position_abs_err"], 2)}
+                                             for st in ("f64", "f32")},
+                                 "as_specified_diverges_at": c1["as_specified"]["f64"]["gpu_divergence_reported_at_tick"]}
+    for k, v in forms.items():
+        if "error" in v:
+            out[k] = {"error": v["error"][:200]}
+        if k in out:
+            out[k]["wall_s"] = v.get("wall_s")
+    return out
+
+
 def run_forms(args, device):
     forms = {}
     for name, fn in (("precision_c2", lambda: form_precision_c2(device)),
                      ("precision_c3", lambda: form_precision_c3(device)),
                      ("batching_c4", lambda: form_batch(device)),
-                     ("gradients_c5", lambda: form_gradients(device))):
+                     ("gradients_c5", lambda: form_gradients(device)),
+                     ("parity", lambda: form_parity(device))):
         if name in args.skip_forms:
             continue
         t0 = time.perf_counter()
@@ -633,10 +794,10 @@ def main(argv=None):
     ap.add_argument("--cpu-ticks", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-forms", default="",
-                    help="comma-separated forms to skip: precision_c2, precision_c3, batching_c4, gradients_c5 "
+                    help="comma-separated forms to skip: precision_c2, precision_c3, batching_c4, gradients_c5, parity "
                          "(all: skip every form)")
     args = ap.parse_args(argv)
-    args.skip_forms = {"precision_c2", "precision_c3", "batching_c4", "gradients_c5"} \
+    args.skip_forms = {"precision_c2", "precision_c3", "batching_c4", "gradients_c5", "parity"} \
         if args.skip_forms == "all" else set(filter(None, args.skip_forms.split(",")))
     if args.impl == "reference":
         return run_reference(args)

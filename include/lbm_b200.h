@@ -100,7 +100,24 @@ typedef struct lbm_config {
     double store_scale;        /* power-of-two scale for F16/BF16 storage (0 -> default 2^12) */
     int32_t device;            /* CUDA device ordinal; < 0: the calling thread's current device */
     int32_t schedule;          /* LBM_SCHEDULE_*: how the kernels of a tick are launched */
+    int32_t particle_rules;    /* LBM_RULES_*: which of the reference's two modules the particle update follows */
+    int32_t reserved;
 } lbm_config;
+
+/* Particle update rules.  The reference has two implementations of the
+ * particle update, picked when the package loads (src/LBMengine.jl:10-24):
+ *   GPU_MODULE  moveParticles! of src/gpu/particles.jl:7-92 (the default):
+ *               v += dt F/m and R += dt v only with coupleForces, Rodrigues
+ *               rotation of the swimming direction with coupleTorques;
+ *   CPU_MODULE  moveParticles! of src/cpu/particles.jl:48-100: v += dP/m and
+ *               w += dL/I from the summed momentum inputs, R += dt v whenever
+ *               v != 0 (whatever coupleForces says), the swimming direction
+ *               never rotates, and the node (slip) velocity is the CPU
+ *               module's bulkVelocity (:21-46).
+ * The fluid step is the same in both (src/gpu/fluids.jl:132-226 and
+ * src/cpu/fluids.jl:377-461). */
+#define LBM_RULES_GPU_MODULE 0
+#define LBM_RULES_CPU_MODULE 1
 
 /* Kernel schedule of a tick.  Results do not depend on it (the per-node
  * arithmetic is the same).
@@ -162,7 +179,27 @@ typedef struct lbm_info {
     int32_t num_particles;
     int32_t bytes_per_population;  /* storage bytes of one population value */
     int64_t device_bytes;          /* device memory held by the handle */
+    int32_t bulk_kernel;           /* LBM_BULK_*: the stream-collide kernel lbm_step launches */
+    int32_t bulk_threads;          /* its threads per CTA */
+    int32_t bulk_stages;           /* shared-memory ring buffers (TMA kernel), else 0 */
+    int32_t reserved;
 } lbm_info;
+
+/* Bulk stream-collide kernel of a tick (results do not depend on it).
+ *   SCALAR  one node per thread (FP64 storage, per-node force fields, rows
+ *           that are not a multiple of 4 nodes or wider than 2048)
+ *   VECTOR  four x-nodes per thread, vector loads and stores
+ *   TMA     as VECTOR, with the loads issued as bulk copies by the Tensor
+ *           Memory Accelerator through a ring of shared-memory buffers; for
+ *           x-rows of 4*2^k <= 128 nodes
+ * lbm_set_bulk_kernel(h, kind, threads, stages): AUTO (the default) is
+ * VECTOR; threads per CTA and ring buffers of the TMA kernel
+ * (0: chosen by the library).  LBM_ERR_UNSUPPORTED where the kind or shape
+ * does not apply. */
+#define LBM_BULK_AUTO 0
+#define LBM_BULK_VECTOR 1
+#define LBM_BULK_TMA 2
+#define LBM_BULK_SCALAR 3
 
 typedef struct lbm_handle lbm_handle;
 
@@ -208,11 +245,15 @@ int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask);
 /* Boundary links of particle `id`: the (cell, direction) pairs of
  * streamingInvasionRegions (bounceBackPrep, src/gpu/aux.jl:187-198), i.e.
  * fluid cells x with x - c_dir solid, as 0-based cell index and 0-based
- * direction index, sorted by (direction, cell).  With cells == NULL only the
- * count is returned in *n. */
+ * direction index, sorted by (direction, cell).  They are read from the
+ * particle's device link list, the one the boundary fix-up uses.  With
+ * cells == NULL only the count is returned in *n. */
 int lbm_get_links(lbm_handle* h, int32_t id, int64_t* cells, int8_t* dirs, int64_t capacity, int64_t* n);
 
 int lbm_get_info(lbm_handle* h, lbm_info* info);
+
+/* Choose the bulk stream-collide kernel (LBM_BULK_*, see lbm_info). */
+int lbm_set_bulk_kernel(lbm_handle* h, int32_t kind, int32_t threads, int32_t stages);
 
 /* Device-time profile of the most recent lbm_step call (CUDA events on the
  * handle's stream; with profiling on, event nodes are captured around every
@@ -248,6 +289,30 @@ int lbm_get_profile(lbm_handle* h, lbm_profile* out);
 #define LBM_KERNEL_PARTICLES 2
 #define LBM_KERNEL_TICK 3
 int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg_ms);
+
+/* Failure detection.  No counterpart in the reference, whose only checks are
+ * the @assert / error sites of its keyword handling
+ * (src/gpu/initMethods.jl:472-473,514,533,540,556).
+ *   - Every bulk stream-collide pass tests the density it forms at each node
+ *     and raises LBM_ERR_NUMERIC from lbm_step (or lbm_batch_step) when it
+ *     is not finite or below -1e-3 (wall nodes hold zero density, as in the
+ *     reference, so zero itself cannot be told apart from a failure).
+ *   - Every wait inside the persistent tick kernel (LBM_SCHEDULE_PERSISTENT)
+ *     gives up after a bounded number of polls and raises LBM_ERR_TIMEOUT.
+ * After either error the model's state is undefined: restore a checkpoint
+ * (lbm_load_state) or destroy the handle; the error word is cleared once
+ * reported, so the handle itself stays usable.
+ *
+ * lbm_set_wait_limit: `polls` bounds every wait of the tick kernel (1 ..
+ * 2^22, the default; a poll sleeps >= 128 ns).  `target_offset` is a test
+ * knob: 1 raises the target of the fix-up items' wait above any count the
+ * kernel can reach, so that wait runs into the limit; 0 in normal use.
+ *
+ * lbm_set_memory_limit: a process-wide cap on the device bytes any one handle
+ * may hold (0, the default: no cap); an allocation beyond it fails with
+ * LBM_ERR_OOM, as a failed cudaMalloc does. */
+int lbm_set_wait_limit(lbm_handle* h, int64_t polls, int32_t target_offset);
+int lbm_set_memory_limit(int64_t bytes);
 
 /* Raw checkpoint of populations + particle FP64 state + tick/time. */
 int lbm_save_state(lbm_handle* h, const char* path);
@@ -294,6 +359,12 @@ int lbm_batch_get_tuning(const lbm_batch* b, lbm_batch_tuning* t);
 /* level 0 off, 1 device time of each lbm_batch_step call (lbm_profile.total_ms) */
 int lbm_batch_set_profiling(lbm_batch* b, int32_t level);
 int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out);
+/* Per-replica status: status[i] = LBM_ERR_NUMERIC for a replica whose density
+ * sentinel fired in some lbm_batch_step (non-finite or negative density, see
+ * "Failure detection" below), else LBM_OK; returns how many replicas
+ * diverged.  A diverged replica does not stop the batch (a parameter sweep
+ * runs on). */
+int lbm_batch_status(const lbm_batch* b, int32_t* status);
 const char* lbm_batch_last_error(const lbm_batch* b);
 void lbm_batch_destroy(lbm_batch* b);
 

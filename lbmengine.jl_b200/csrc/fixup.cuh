@@ -279,7 +279,8 @@ __device__ __forceinline__ bool fixup_body(const StepArgs& a, const long long b)
     grid_dep_wait();
     for (int l = tid; l < nlist; l += NT) {
         const int item = s_list[l];
-        dst[(item & 31) * N + s_cell[item >> 5]] = SS::enc(s_val[l], R(a.scale));
+        dst[(item & 31) * N + s_cell[item >> 5]] =
+            SS::enc_sr(s_val[l], R(a.scale), (unsigned)s_cell[item >> 5], item & 31);
     }
     if (!is_part) return true;
     // fixed-order reduction: butterfly inside warps, warps summed in order

@@ -36,6 +36,23 @@ constexpr int kLinkOcParams = 8;   // particles whose (link_off, link_cap) the f
 // device error word bits
 constexpr int kErrLinkOverflow = 1;
 constexpr int kErrIntervalOverflow = 2;
+constexpr int kErrSpinTimeout = 4;  // a bounded wait gave up (tick kernel, TMA ring)
+constexpr int kErrNumeric = 8;
+
+// Density sentinel of the bulk pass: rho^n is not finite or below -1e-3.  Wall
+// nodes hold zero density (their populations are reset to f = 0, fluids.jl:154),
+// so the test cannot stop at zero.
+template <class R>
+__device__ __forceinline__ bool bad_density(R rho) {
+    return !(rho >= R(-1e-3) && rho <= R(1e30));
+}
+
+// raise kErrNumeric once per warp if any of its threads saw a bad density
+// (every thread of the warp must call it)
+__device__ __forceinline__ void report_density(bool bad, int* err) {
+    const unsigned any = __ballot_sync(0xffffffffu, bad);
+    if (any && (threadIdx.x & 31) == __ffs(any) - 1) atomicOr(err, kErrNumeric);
+}
 
 struct GridDesc {
     int n[3];        // nodes per axis
@@ -428,6 +445,7 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
     grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
     NodeState<L, ST, TRT> s;
     load_collide<L, ST, TRT>(a, cell, valid, s);
+    report_density(valid && bad_density(s.rho), a.err);
     if (!valid) return;
     const int xs[3] = {x == 0 ? nx - 1 : x - 1, x, x == nx - 1 ? 0 : x + 1};
     const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
@@ -437,7 +455,7 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int t = xs[L::cx(i) + 1] + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
-        dst[i * N + t] = SS::enc(s.g[i], R(1));
+        dst[i * N + t] = SS::enc_sr(s.g[i], R(1), (unsigned)t, i);
     }
 }
 
@@ -455,7 +473,8 @@ template <> struct Vec4<ST_F32> {
         const float4 q = __ldcs(reinterpret_cast<const float4*>(static_cast<const float*>(base) + cell0));
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
+    // values of direction `dir` for cells cell0 .. cell0+3 (cell0 a multiple of 4)
+    static __device__ __forceinline__ void store(void* base, int cell0, int, float a0, float a1, float a2, float a3) {
         // streaming (evict-first) store: the next read of the line is a tick away,
         // after the pass has streamed far more than L2 through the cache
         __stcs(reinterpret_cast<float4*>(static_cast<float*>(base) + cell0), make_float4(a0, a1, a2, a3));
@@ -468,9 +487,13 @@ template <> struct Vec4<ST_F16> {
         const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
-        const __half2 lo = __floats2half2_rn(a0, a1);
-        const __half2 hi = __floats2half2_rn(a2, a3);
+    static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
+                                                 float a3) {
+        const unsigned key = (unsigned)cell0 * kDitherCell;  // stochastic rounding (storage.cuh)
+        const __half2 lo = __floats2half2_rn(round_dither<13>(a0, key, dither_mul(dir, 0)),
+                                             round_dither<13>(a1, key, dither_mul(dir, 1)));
+        const __half2 hi = __floats2half2_rn(round_dither<13>(a2, key, dither_mul(dir, 2)),
+                                             round_dither<13>(a3, key, dither_mul(dir, 3)));
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
@@ -484,9 +507,13 @@ template <> struct Vec4<ST_BF16> {
         const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.y));
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
-    static __device__ __forceinline__ void store(void* base, int cell0, float a0, float a1, float a2, float a3) {
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(a0, a1);
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(a2, a3);
+    static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
+                                                 float a3) {
+        const unsigned key = (unsigned)cell0 * kDitherCell;  // stochastic rounding (storage.cuh)
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(round_dither<16>(a0, key, dither_mul(dir, 0)),
+                                                        round_dither<16>(a1, key, dither_mul(dir, 1)));
+        const __nv_bfloat162 hi = __floats2bfloat162_rn(round_dither<16>(a2, key, dither_mul(dir, 2)),
+                                                        round_dither<16>(a3, key, dither_mul(dir, 3)));
         uint2 q;
         q.x = *reinterpret_cast<const unsigned*>(&lo);
         q.y = *reinterpret_cast<const unsigned*>(&hi);
@@ -540,8 +567,10 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
         g[3][i] = v[3];
     }
     const R Fx = a.kf.F[0], Fy = a.kf.F[1], Fz = a.kf.F[2];
+    bool bad = false;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) collide<L, R, TRT>(a, g[k], Fx, Fy, Fz, false);
+    for (int k = 0; k < 4; ++k) bad |= bad_density(collide<L, R, TRT>(a, g[k], Fx, Fy, Fz, false));
+    report_density(valid && bad, a.err);
     // the value of each +-x direction that leaves this thread's 4-node segment
     if (row < a.vrows) {
 #pragma unroll
@@ -560,11 +589,11 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
     for (int i = 0; i < Q; ++i) {
         const int t0 = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
         if (L::cx(i) == 0) {
-            Vec4<ST>::store(a.dstq[i], t0, g[0][i], g[1][i], g[2][i], g[3][i]);
+            Vec4<ST>::store(a.dstq[i], t0, i, g[0][i], g[1][i], g[2][i], g[3][i]);
         } else if (L::cx(i) == 1) {
-            Vec4<ST>::store(a.dstq[i], t0, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i]);
+            Vec4<ST>::store(a.dstq[i], t0, i, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i]);
         } else {
-            Vec4<ST>::store(a.dstq[i], t0, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right]);
+            Vec4<ST>::store(a.dstq[i], t0, i, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right]);
         }
     }
 }

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <chrono>
 #include <mutex>
 #include <string>
@@ -33,9 +34,12 @@ struct Graph {
 };
 
 constexpr int kGraphSteps = 16;  // ticks per CUDA graph of a batch
-// ticks per CUDA graph of one model: each graph ends by joining the side
-// stream (the last particle update), a bubble that longer graphs amortise
-constexpr int kModelGraphTicks = 64;
+// Ticks per CUDA graph of one model, longest first: a call of n ticks replays
+// the longest graphs that fit, so every tick count runs from graphs.  Each
+// graph ends by joining the side stream (the last particle update), a bubble
+// that longer graphs amortise.
+constexpr int kModelGraphSizes[4] = {64, 16, 4, 1};
+constexpr int kModelGraphTicks = kModelGraphSizes[0];
 
 }  // namespace
 
@@ -62,6 +66,10 @@ struct lbm_handle {
     bool part_pending = false;
     // vector bulk pass: tiles of vrows full x-rows, vblock threads per tile
     int vrows = 0, vnt1 = 0, vblock = 0;
+    // TMA bulk pass (bulk_tma.cuh): its launch shape, valid when tma_ok
+    int bulk_kind = LBM_BULK_AUTO;
+    TmaShape tma{};
+    bool tma_ok = false;
     long long vtiles = 0;
     std::vector<unsigned char> vnear;  // static near flags of the tiles (walls)
     unsigned char* d_vnear = nullptr;
@@ -75,6 +83,8 @@ struct lbm_handle {
     StepArgs* d_targs = nullptr;      // [2]: by source buffer
     ParticleArgs* d_pargs = nullptr;  // [2]
     TickCounters* d_tq = nullptr;
+    long long spin_limit = kSpinLimit;  // polls before a wait of the tick kernel gives up
+    int wait_extra = 0;                 // test knob: added to the fix-up items' wait target
     void* pop[2] = {nullptr, nullptr};
     int cur = 0;
     double* d_coord[3] = {nullptr, nullptr, nullptr};
@@ -106,8 +116,8 @@ struct lbm_handle {
     // time
     long long tick = 0;
     double time = 0;
-    // graphs of kModelGraphTicks ticks: [profiling][starting buffer]
-    Graph graphs[2][2];
+    // graphs of kModelGraphSizes[k] ticks: [profiling][starting buffer][k]
+    Graph graphs[2][2][4];
     // profiling: per graph slot, events before/after the bulk kernel, after
     // the fix-up and after the particle kernel; plus the whole call
     int profiling = 0;  // 0 off, 1 whole-call time, 2 also per-kernel event nodes
@@ -143,8 +153,18 @@ int set_err(lbm_handle* h, int code, const std::string& msg) {
         }                                                                                              \
     } while (0)
 
+// process-wide cap on the device bytes one handle or batch may hold (0: none)
+std::atomic<long long> g_mem_limit{0};
+
 template <class P>
 int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
+    const long long cap = g_mem_limit.load();
+    if (cap > 0 && (long long)(h->device_bytes + bytes) > cap) {
+        *p = nullptr;
+        return set_err(h, LBM_ERR_OOM, "device allocation of " + std::to_string(bytes) +
+                                           " bytes would exceed the memory limit of " + std::to_string(cap) +
+                                           " bytes (lbm_set_memory_limit)");
+    }
     cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -225,14 +245,38 @@ int ensure_tmp(lbm_handle* h, size_t bytes) {
 
 void drop_graphs(lbm_handle* h) {
     h->tick_ready = false;  // the tick kernel's maps and arguments are rebuilt with the graphs
-    for (auto& row : h->graphs)
-        for (auto& gr : row) {
-            if (gr.exec) cudaGraphExecDestroy(gr.exec);
-            gr.exec = nullptr;
-        }
+    for (auto& prof : h->graphs)
+        for (auto& row : prof)
+            for (auto& gr : row) {
+                if (gr.exec) cudaGraphExecDestroy(gr.exec);
+                gr.exec = nullptr;
+            }
 }
 
-StepArgs step_args(const lbm_handle* h, int src) {
+template <class L>
+void lattice_vectors_of(int* cx, int* cy, int* cz, int* q) {
+    *q = L::Q;
+    for (int i = 0; i < L::Q; ++i) {
+        cx[i] = L::cx(i);
+        cy[i] = L::cy(i);
+        cz[i] = L::cz(i);
+    }
+}
+
+// lattice vectors of a velocity set into fixed arrays (no host heap use, so
+// that the allocation-free entry point can build its arguments too)
+void lattice_vectors(int lattice, int* cx, int* cy, int* cz, int* q) {
+    switch (lattice) {
+        case LBM_D2Q9: lattice_vectors_of<D2Q9>(cx, cy, cz, q); break;
+        case LBM_D3Q15: lattice_vectors_of<D3Q15>(cx, cy, cz, q); break;
+        case LBM_D3Q19: lattice_vectors_of<D3Q19>(cx, cy, cz, q); break;
+        default: lattice_vectors_of<D3Q27>(cx, cy, cz, q); break;
+    }
+}
+
+// Kernel arguments of one tick from buffer `src`, with the fix-up's
+// momentum-exchange partials in `partial`.  Uses no host heap.
+StepArgs make_step_args(const lbm_handle* h, int src, double* partial) {
     StepArgs a{};
     a.src = h->pop[src];
     a.dst = h->pop[1 - src];
@@ -262,7 +306,7 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.vtiles = h->vtiles;
     a.nbox = h->d_nbox[src];
     a.vnear = h->d_vnear;
-    a.partial = h->d_partial;
+    a.partial = partial;
     a.err = h->d_err;
     a.rho0 = h->rho0;
     a.scale = h->scale;
@@ -286,15 +330,16 @@ StepArgs step_args(const lbm_handle* h, int src) {
     a.gK0 = (h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k) * h->scale;
     a.gkA = kodd;
     a.gkB = keven;
-    const HostLattice hl = host_lattice(h->lattice);
+    int cx[27], cy[27], cz[27], q = 0;
+    lattice_vectors(h->lattice, cx, cy, cz, &q);
     const size_t esz = storage_bytes(h->storage);
     for (int i = 0; i < 27; ++i) {
         a.gA[i] = a.gB[i] = 0.0;
         a.srcq[i] = nullptr;
         a.dstq[i] = nullptr;
     }
-    for (int i = 0; i < hl.q; ++i) {
-        const double cF = hl.cx[i] * h->F[0] + hl.cy[i] * h->F[1] + hl.cz[i] * h->F[2];
+    for (int i = 0; i < q; ++i) {
+        const double cF = cx[i] * h->F[0] + cy[i] * h->F[1] + cz[i] * h->F[2];
         a.gA[i] = kodd * cF;
         a.gB[i] = keven * cF;
         a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
@@ -305,13 +350,62 @@ StepArgs step_args(const lbm_handle* h, int src) {
     return a;
 }
 
+StepArgs step_args(const lbm_handle* h, int src) { return make_step_args(h, src, h->d_partial); }
+
 bool use_vector_bulk(const lbm_handle* h) {
     return h->ops.bulk_v4 != nullptr && h->force_mode != LBM_FORCE_FIELD && h->vrows > 0;
 }
 
+// the TMA bulk pass is used where its shape is valid and the caller asked for it
+bool use_tma_bulk(const lbm_handle* h) {
+    return h->tma_ok && h->bulk_kind == LBM_BULK_TMA && use_vector_bulk(h);
+}
+
+// Launch shape of the TMA bulk pass for `threads` threads per CTA and
+// `stages` ring buffers (0: chosen here); false where it does not apply:
+// rows of nx = 4 RT nodes with RT a power of two up to 32 (a row is a
+// shuffle segment of a warp), 16-byte aligned rows, no per-node force field.
+bool choose_tma(lbm_handle* h, int threads, int stages, TmaShape* out) {
+    if (!h->ops.bulk_tma || !h->ops.bulk_tma_fn || h->force_mode == LBM_FORCE_FIELD) return false;
+    const int nx = h->n[0], ny = h->n[1], esz = storage_bytes(h->storage);
+    if (nx % 4 != 0) return false;
+    const int RT = nx / 4;
+    if (RT > 32 || (RT & (RT - 1)) != 0 || (nx * esz) % 16 != 0) return false;
+    if (threads <= 0) threads = esz == 4 ? 256 : 512;
+    if (threads > 512 || threads % 32 != 0 || threads % RT != 0) return false;
+    int rows = threads / RT;
+    while (rows > ny && rows * RT > 32) rows /= 2;  // no more rows than the grid has
+    threads = rows * RT;
+    if (threads % 32 != 0) return false;
+    const long long stage_bytes = (long long)h->q * rows * nx * esz;
+    if (stage_bytes >= (1 << 20)) return false;  // an mbarrier's transaction count
+    if (stages <= 0) stages = (int)std::min<long long>(kTmaMaxStages, (200 * 1024) / stage_bytes);
+    if (stages < 2 || stages > kTmaMaxStages) return false;
+    const int smem = tma_smem_bytes(h->q, nx, rows, stages, esz);
+    if (smem > 227 * 1024) return false;
+    if (cudaFuncSetAttribute(h->ops.bulk_tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h->ops.bulk_tma_fn, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    const long long tiles = (long long)((ny + rows - 1) / rows) * h->n[2];
+    out->rows = rows;
+    out->stages = stages;
+    out->smem = smem;
+    out->grid = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)per_sm * sms));
+    return true;
+}
+
 // the bulk pass over all tiles
 void launch_bulk(const lbm_handle* h, const StepArgs& a, cudaStream_t s) {
-    if (use_vector_bulk(h))
+    if (use_tma_bulk(h))
+        h->ops.bulk_tma(a, h->tma, s);
+    else if (use_vector_bulk(h))
         h->ops.bulk_v4(a, h->vtiles, h->vblock, s);
     else
         h->ops.bulk(a, (unsigned)h->g.ntiles, dim3(h->g.t[0], h->g.t[1], h->g.t[2]), s);
@@ -439,6 +533,8 @@ int prepare_tick(lbm_handle* h) {
     h->items.nc = (long long)cm.size();
     h->items.nd = (long long)dm.size();
     h->items.d_test = 1;
+    h->items.spin_limit = h->spin_limit;
+    h->items.wait_extra = h->wait_extra;
     h->tick_ready = true;
     return LBM_OK;
 }
@@ -550,13 +646,13 @@ void join_particles(lbm_handle* h) {
     }
 }
 
-int build_graph(lbm_handle* h, int start) {
-    Graph& gr = h->graphs[h->profiling >= 2 ? 1 : 0][start];
+int build_graph(lbm_handle* h, int start, int size_idx) {
+    Graph& gr = h->graphs[h->profiling >= 2 ? 1 : 0][start][size_idx];
     if (gr.exec) return LBM_OK;
     cudaGraph_t graph = nullptr;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int b = start;
-    for (int s = 0; s < kModelGraphTicks; ++s) {
+    for (int s = 0; s < kModelGraphSizes[size_idx]; ++s) {
         enqueue_tick(h, b, s);
         b = 1 - b;
     }
@@ -572,17 +668,40 @@ int build_graph(lbm_handle* h, int start) {
         gr.exec = nullptr;
         return set_err(h, LBM_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
     }
+    // upload now: a graph's first launch otherwise pays for it
+    CUDA_TRY(h, cudaGraphUpload(gr.exec, h->stream));
     return LBM_OK;
 }
 
+// every graph of the current profiling level, for both starting buffers, so
+// that no call after the first captures or instantiates
+int ensure_graphs(lbm_handle* h) {
+    for (int start = 0; start < 2; ++start)
+        for (int k = 0; k < 4; ++k) {
+            const int rc = build_graph(h, start, k);
+            if (rc) return rc;
+        }
+    return LBM_OK;
+}
+
+// Read (and clear) the device error word after the work of a call.  The state
+// of the model after any of these errors is undefined: restore a checkpoint
+// (lbm_load_state) or destroy the handle.
 int check_device_error(lbm_handle* h) {
     int err = 0;
     CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (err == 0) return LBM_OK;
+    CUDA_TRY(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (err & kErrLinkOverflow) return set_err(h, LBM_ERR_STATE, "particle boundary links exceeded their capacity");
     if (err & kErrIntervalOverflow) return set_err(h, LBM_ERR_STATE, "particle solid box exceeded its capacity");
     if (err & kErrSpinTimeout) return set_err(h, LBM_ERR_TIMEOUT, "a wait inside the tick kernel gave up");
-    return LBM_OK;
+    if (err & kErrNumeric)
+        return set_err(h, LBM_ERR_NUMERIC,
+                       "non-finite or negative density on the device (the simulation diverged near tick " +
+                           std::to_string(h->tick) + ")");
+    return set_err(h, LBM_ERR_STATE, "unknown device error word " + std::to_string(err));
 }
 
 // CTA tile: full x-rows up to 256 nodes (x-wrap stays inside the CTA)
@@ -821,6 +940,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         return set_err(nullptr, LBM_ERR_INVALID, "force density does not have consistent dimensions!");
     if (!cfg->compressible && cfg->rho_init)
         return set_err(nullptr, LBM_ERR_UNSUPPORTED, "incompressible equilibrium with a non-uniform initial density");
+    if (cfg->particle_rules != LBM_RULES_GPU_MODULE && cfg->particle_rules != LBM_RULES_CPU_MODULE)
+        return set_err(nullptr, LBM_ERR_INVALID, "unknown particle rules");
 
     lbm_handle* h = new lbm_handle();
     h->device = device;
@@ -894,6 +1015,7 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
             TRY(set_err(h, LBM_ERR_CUDA, "occupancy query failed"));
         h->tick_grid = (unsigned)std::max(0, per_sm * sms);
     }
+    h->tma_ok = choose_tma(h, 0, 0, &h->tma);
     const size_t pop_bytes = (size_t)N * h->q * storage_bytes(h->storage);
     TRY(dev_alloc(h, &h->pop[0], pop_bytes));
     TRY(dev_alloc(h, &h->pop[1], pop_bytes));
@@ -1121,20 +1243,20 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
         const int rc = prepare_tick(h);
         if (rc) return rc;
     }
+    if (nsteps > 0) {
+        const int rc = ensure_graphs(h);
+        if (rc) return rc;
+    }
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_begin, h->stream));
     int64_t done = 0;
     int slots_used = 0;
-    while (nsteps - done >= kModelGraphTicks) {
-        int rc = build_graph(h, h->cur);
-        if (rc) return rc;
-        CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling >= 2 ? 1 : 0][h->cur].exec, h->stream));
-        done += kModelGraphTicks;  // kModelGraphTicks is even: the buffer parity is unchanged
-        slots_used = kModelGraphTicks;
-    }
-    for (int s = 0; done < nsteps; ++done, ++s) {
-        enqueue_tick(h, h->cur, s % kModelGraphTicks);
-        h->cur = 1 - h->cur;
-        slots_used = std::max(slots_used, std::min(s + 1, kModelGraphTicks));
+    while (done < nsteps) {
+        int k = 0;
+        while (kModelGraphSizes[k] > nsteps - done) ++k;  // the last size is 1
+        CUDA_TRY(h, cudaGraphLaunch(h->graphs[h->profiling >= 2 ? 1 : 0][h->cur][k].exec, h->stream));
+        done += kModelGraphSizes[k];
+        if (kModelGraphSizes[k] & 1) h->cur = 1 - h->cur;
+        slots_used = std::max(slots_used, kModelGraphSizes[k]);
     }
     join_particles(h);
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_end, h->stream));
@@ -1198,6 +1320,49 @@ int lbm_set_profiling(lbm_handle* h, int32_t on) {
 int lbm_get_profile(lbm_handle* h, lbm_profile* out) {
     if (!h || !out) return set_err(h, LBM_ERR_INVALID, "null argument");
     *out = h->prof;
+    return LBM_OK;
+}
+
+int lbm_set_wait_limit(lbm_handle* h, int64_t polls, int32_t target_offset) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (polls < 1 || polls > kSpinLimit)
+        return set_err(h, LBM_ERR_INVALID, "the wait limit must lie in [1, " + std::to_string(kSpinLimit) + "] polls");
+    if (target_offset < 0 || target_offset > 1) return set_err(h, LBM_ERR_INVALID, "target_offset must be 0 or 1");
+    BIND(h);
+    h->spin_limit = polls;
+    h->wait_extra = target_offset;
+    drop_graphs(h);  // the graphs hold the tick kernel's arguments
+    return LBM_OK;
+}
+
+int lbm_set_bulk_kernel(lbm_handle* h, int32_t kind, int32_t threads, int32_t stages) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (kind != LBM_BULK_AUTO && kind != LBM_BULK_VECTOR && kind != LBM_BULK_TMA)
+        return set_err(h, LBM_ERR_INVALID, "unknown bulk kernel");
+    BIND(h);
+    if (kind == LBM_BULK_VECTOR && !use_vector_bulk(h))
+        return set_err(h, LBM_ERR_UNSUPPORTED, "the vector bulk kernel does not apply to this model");
+    if (kind != LBM_BULK_VECTOR) {
+        TmaShape sh{};
+        if (!choose_tma(h, threads, stages, &sh)) {
+            if (kind == LBM_BULK_TMA)
+                return set_err(h, LBM_ERR_UNSUPPORTED,
+                               "the TMA bulk kernel does not apply to this model or launch shape (x-rows of 4*2^k "
+                               "<= 128 nodes, 16-byte aligned rows, no force field, shared memory <= 227 KB)");
+            h->tma_ok = false;
+        } else {
+            h->tma = sh;
+            h->tma_ok = true;
+        }
+    }
+    h->bulk_kind = kind;
+    drop_graphs(h);
+    return LBM_OK;
+}
+
+int lbm_set_memory_limit(int64_t bytes) {
+    if (bytes < 0) return set_err(nullptr, LBM_ERR_INVALID, "the memory limit must be non-negative");
+    g_mem_limit.store(bytes);
     return LBM_OK;
 }
 
@@ -1390,27 +1555,28 @@ int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask) {
     return LBM_OK;
 }
 
-// boundary links of the device solid region: fluid cells x with x - c_j solid
-// (periodic shift, bounceBackPrep), sorted by (direction, cell)
+// Boundary links of a particle as the fix-up kernel sees them: the entries
+// (fluid cell, direction mask) of its device link list, bit j of the mask set
+// where x - c_j is solid (the streamingInvasionRegions of bounceBackPrep,
+// src/gpu/aux.jl:187-198), expanded to (cell, direction) pairs sorted by
+// (direction, cell).
 int lbm_get_links(lbm_handle* h, int32_t id, int64_t* cells, int8_t* dirs, int64_t capacity, int64_t* n) {
     if (!h || !n) return set_err(h, LBM_ERR_INVALID, "null argument");
-    std::vector<uint8_t> S(h->N);
-    int rc = lbm_get_mask(h, id, S.data());
-    if (rc) return rc;
-    const HostLattice hl = host_lattice(h->lattice);
+    BIND(h);
+    if (id < 1 || id > (int)h->hparts.size()) return set_err(h, LBM_ERR_INVALID, "no such particle");
+    ParticleDev P;
+    CUDA_TRY(h, cudaMemcpyAsync(&P, h->d_parts + (id - 1), sizeof(P), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (P.relink) return set_err(h, LBM_ERR_STATE, "the particle's link list awaits its rebuild");
+    std::vector<int2> ent(std::max(0, P.nlinks));
+    if (!ent.empty())
+        CUDA_TRY(h, cudaMemcpyAsync(ent.data(), h->d_links + P.link_off, sizeof(int2) * ent.size(),
+                                    cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     std::vector<std::vector<int64_t>> per(h->q);
-    for (long long y = 0; y < h->N; ++y) {
-        if (!S[y]) continue;
-        const int x0 = (int)(y % h->n[0]), y0 = (int)((y / h->n[0]) % h->n[1]);
-        const int z0 = (int)(y / ((long long)h->n[0] * h->n[1]));
-        for (int j = 1; j < hl.q; ++j) {
-            const int xx = (x0 + hl.cx[j] + h->n[0]) % h->n[0];
-            const int yy = (y0 + hl.cy[j] + h->n[1]) % h->n[1];
-            const int zz = (z0 + hl.cz[j] + h->n[2]) % h->n[2];
-            const long long x = xx + (long long)h->n[0] * (yy + (long long)h->n[1] * zz);
-            if (!S[x]) per[j].push_back(x);
-        }
-    }
+    for (const int2& e : ent)
+        for (int j = 1; j < h->q; ++j)
+            if ((unsigned)e.y >> j & 1u) per[j].push_back(e.x);
     int64_t k = 0;
     for (int j = 0; j < h->q; ++j) {
         std::sort(per[j].begin(), per[j].end());
@@ -1440,6 +1606,15 @@ int lbm_get_info(lbm_handle* h, lbm_info* info) {
     info->num_particles = (int32_t)h->hparts.size();
     info->bytes_per_population = storage_bytes(h->storage);
     info->device_bytes = (int64_t)h->device_bytes;
+    if (use_tma_bulk(h)) {
+        info->bulk_kernel = LBM_BULK_TMA;
+        info->bulk_threads = h->tma.rows * (h->n[0] / 4);
+        info->bulk_stages = h->tma.stages;
+    } else {
+        info->bulk_kernel = use_vector_bulk(h) ? LBM_BULK_VECTOR : LBM_BULK_SCALAR;
+        info->bulk_threads = use_vector_bulk(h) ? h->vblock : h->g.t[0] * h->g.t[1];
+        info->bulk_stages = 0;
+    }
     return LBM_OK;
 }
 
@@ -1550,91 +1725,6 @@ int noalloc_scratch(lbm_handle* h, double** out) {
     return LBM_OK;
 }
 
-template <class L>
-void noalloc_lattice_of(int* cx, int* cy, int* cz, int* q) {
-    *q = L::Q;
-    for (int i = 0; i < L::Q; ++i) {
-        cx[i] = L::cx(i);
-        cy[i] = L::cy(i);
-        cz[i] = L::cz(i);
-    }
-}
-
-// the StepArgs of step_args(), built without host heap use and with the
-// partial sums redirected to `partial`
-StepArgs noalloc_step_args(const lbm_handle* h, int src, double* partial) {
-    int cx[27], cy[27], cz[27], q = 0;
-    switch (h->lattice) {
-        case LBM_D2Q9: noalloc_lattice_of<D2Q9>(cx, cy, cz, &q); break;
-        case LBM_D3Q15: noalloc_lattice_of<D3Q15>(cx, cy, cz, &q); break;
-        case LBM_D3Q19: noalloc_lattice_of<D3Q19>(cx, cy, cz, &q); break;
-        default: noalloc_lattice_of<D3Q27>(cx, cy, cz, &q); break;
-    }
-    StepArgs a{};
-    a.src = h->pop[src];
-    a.dst = h->pop[1 - src];
-    a.g = h->g;
-    for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
-    a.tilebits = h->d_tilebits;
-    a.words = h->words;
-    a.nparts = (int)h->hparts.size();
-    a.wall = h->d_wall;
-    a.uw = h->d_uw;
-    a.ffield = h->d_ffield;
-    a.parts = h->d_parts;
-    a.ivl = h->d_ivl;
-    a.links = h->d_links;
-    a.wlinks = h->d_wlinks;
-    a.wnodes = h->d_wnodes;
-    a.nwlinks = h->nwlinks;
-    a.nwnodes = h->nwnodes;
-    a.maxchunks = h->maxchunks;
-    a.vrows = h->vrows;
-    a.vnt1 = h->vnt1;
-    a.vtiles = h->vtiles;
-    a.nbox = h->d_nbox[src];
-    a.vnear = h->d_vnear;
-    a.partial = partial;
-    a.err = h->d_err;
-    a.rho0 = h->rho0;
-    a.scale = h->scale;
-    a.inv_scale = 1.0 / h->scale;
-    a.omega = h->dt / h->tau;
-    a.omega_p = h->dt / h->tau;
-    a.omega_m = h->trt ? h->dt / h->tau_minus : 0.0;
-    a.guo_k = h->dt * (1 - h->dt / (2 * h->tau));
-    a.guo_kp = a.guo_k;
-    a.guo_km = h->trt ? h->dt * (1 - h->dt / (2 * h->tau_minus)) : 0.0;
-    for (int k = 0; k < 3; ++k) a.F[k] = h->F[k];
-    a.half_dt = 0.5 * h->dt;
-    a.coeff = std::pow(h->dx, h->dims) / h->dt;
-    a.force_mode = h->force_mode;
-    a.incompressible = h->incompressible;
-    a.rho_inc = h->rho_inc;
-    // in storage units: collide() works on g' = S (f/w - rho0)
-    const double kodd = (h->trt ? 3.0 * a.guo_km : 3.0 * a.guo_k) * h->scale;
-    const double keven = (h->trt ? 9.0 * a.guo_kp : 9.0 * a.guo_k) * h->scale;
-    a.gK0 = (h->trt ? -3.0 * a.guo_kp : -3.0 * a.guo_k) * h->scale;
-    a.gkA = kodd;
-    a.gkB = keven;
-    const size_t esz = storage_bytes(h->storage);
-    for (int i = 0; i < 27; ++i) {
-        a.gA[i] = a.gB[i] = 0.0;
-        a.srcq[i] = nullptr;
-        a.dstq[i] = nullptr;
-    }
-    for (int i = 0; i < q; ++i) {
-        const double cF = cx[i] * h->F[0] + cy[i] * h->F[1] + cz[i] * h->F[2];
-        a.gA[i] = kodd * cF;
-        a.gB[i] = keven * cF;
-        a.srcq[i] = static_cast<const char*>(a.src) + (size_t)i * h->N * esz;
-        a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
-    }
-    a.trt = h->trt;
-    fill_collide_consts(a);
-    return a;
-}
-
 }  // namespace
 
 extern "C" {
@@ -1665,7 +1755,7 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
     const long long nb = fixup_blocks(h);
     const int np = (int)h->hparts.size();
     for (int64_t s = 0; s < nsteps; ++s) {
-        const StepArgs a = noalloc_step_args(h, h->cur, scratch);
+        const StepArgs a = make_step_args(h, h->cur, scratch);
         pa.nbox_out[0] = h->d_nbox[h->cur];
         launch_bulk(h, a, h->stream);
         if (nb > 0) h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, false, fixup_walk(h));
@@ -1709,6 +1799,7 @@ struct lbm_batch {
     ParticleArgs* d_pargs = nullptr;  // [2][n]
     TickCounters* d_tq = nullptr;     // [0] main-stream launches, [1] side-stream launches
     int* d_err = nullptr;             // [n] per replica, plus one for the queue waits
+    std::vector<int> diverged;        // [n] replicas whose density sentinel fired (sticky)
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
     int profiling = 0;
     cudaEvent_t t_begin = nullptr, t_end = nullptr;
@@ -1849,6 +1940,7 @@ TickItems batch_items(const lbm_batch* b, bool a, bool bb, bool c, bool d, int d
     it.nc = c ? b->nc : 0;
     it.nd = d ? b->nd : 0;
     it.d_test = d_test;
+    it.spin_limit = kSpinLimit;
     // items past the enabled phases are addressed from the start of their map
     if (!a) it.amap = nullptr;
     return it;
@@ -1922,6 +2014,15 @@ int batch_check(lbm_batch* b) {
     std::vector<int> err(n + 1, 0);
     BCUDA_TRY(b, cudaMemcpyAsync(err.data(), b->d_err, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, b->stream));
     BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    bool any = false;
+    for (size_t r = 0; r <= n; ++r) any = any || err[r] != 0;
+    if (any) {  // reported below; the words start from zero again
+        BCUDA_TRY(b, cudaMemsetAsync(b->d_err, 0, sizeof(int) * (n + 1), b->stream));
+        BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    }
+    b->diverged.resize(n, 0);
+    for (size_t r = 0; r < n; ++r)
+        if (err[r] & kErrNumeric) b->diverged[r] = 1;  // a sweep goes on; lbm_batch_status reports them
     if (err[n] & kErrSpinTimeout) return bset_err(b, LBM_ERR_TIMEOUT, "a wait inside the tick kernel gave up");
     for (size_t r = 0; r < n; ++r) {
         if (err[r] & kErrLinkOverflow)
@@ -2185,6 +2286,7 @@ int lbm_batch_autotune(lbm_batch* b, int32_t ticks, lbm_batch_tuning* results, i
                 }
         }
     const lbm_batch_tuning keep = b->tuning;
+    const std::vector<int> keep_diverged = b->diverged;  // the candidates' ticks are undone
     int best = -1;
     for (size_t i = 0; i < cand.size(); ++i) {
         if (cand[i].tile_order != b->tuning.tile_order) {
@@ -2204,6 +2306,7 @@ int lbm_batch_autotune(lbm_batch* b, int32_t ticks, lbm_batch_tuning* results, i
     }
     dev_free(save);
     batch_drop_graphs(b);
+    b->diverged = keep_diverged;
     if (rc || best < 0) {
         b->tuning = keep;
         batch_free_items(b);
@@ -2235,6 +2338,17 @@ int lbm_batch_get_profile(const lbm_batch* b, lbm_profile* out) {
     if (!b || !out) return LBM_ERR_INVALID;
     *out = b->prof;
     return LBM_OK;
+}
+
+int lbm_batch_status(const lbm_batch* b, int32_t* status) {
+    if (!b) return set_err(nullptr, LBM_ERR_INVALID, "null batch");
+    int count = 0;
+    for (size_t r = 0; r < b->reps.size(); ++r) {
+        const bool d = r < b->diverged.size() && b->diverged[r];
+        if (status) status[r] = d ? LBM_ERR_NUMERIC : LBM_OK;
+        count += d ? 1 : 0;
+    }
+    return count;
 }
 
 const char* lbm_batch_last_error(const lbm_batch* b) { return b ? b->err.c_str() : g_global_err.c_str(); }

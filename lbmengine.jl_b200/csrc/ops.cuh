@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "kernels.cuh"
+#include "bulk_tma.cuh"
 #include "fixup.cuh"
 #include "particles.cuh"
 #include "aux_kernels.cuh"
@@ -28,6 +29,8 @@ struct Ops {
     void (*mask)(const MaskArgs&, cudaStream_t);
     // vector bulk pass over all tiles, CTAs of `block` threads (64..512); null for FP64
     void (*bulk_v4)(const StepArgs&, long long tiles, int block, cudaStream_t);
+    // the same pass with TMA bulk loads through a shared-memory ring (bulk_tma.cuh); null for FP64
+    void (*bulk_tma)(const StepArgs&, const TmaShape&, cudaStream_t);
     // one persistent kernel per tick over the A/B/C/D item queue (tick.cuh)
     void (*tick)(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
                  int* err, unsigned grid, cudaStream_t);
@@ -37,6 +40,7 @@ struct Ops {
     void (*adjoint)(const AdjArgs&, cudaStream_t);
     void (*adjoint_init)(const AdjArgs&, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
+    const void* bulk_tma_fn;
     const void* fixup_fn;
     const void* tick_fn;
 };
@@ -80,6 +84,11 @@ struct OpsImpl {
             else k_bulk_v4<L, ST, TRT, 512><<<g, 512, 0, s>>>(a);
         }
     }
+    static void bulk_tma(const StepArgs& a, const TmaShape& sh, cudaStream_t s) {
+        if constexpr (ST != ST_F64)
+            k_bulk_tma<L, ST, TRT><<<(unsigned)sh.grid, (unsigned)(sh.rows * (a.g.n[0] / 4)), (size_t)sh.smem, s>>>(
+                a, sh.rows, sh.stages);
+    }
     static void tick(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
                      int* err, unsigned grid, cudaStream_t s) {
         if constexpr (ST != ST_F64) k_tick<L, ST, TRT><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
@@ -114,6 +123,9 @@ struct OpsImpl {
         o.init = init;
         o.mask = mask;
         o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
+        o.bulk_tma = ST == ST_F64 ? nullptr : bulk_tma;
+        o.bulk_tma_fn = nullptr;
+        if constexpr (ST != ST_F64) o.bulk_tma_fn = (const void*)k_bulk_tma<L, ST, TRT>;
         o.tick = ST == ST_F64 ? nullptr : tick;
         o.bulk_batch = ST == ST_F64 ? nullptr : bulk_batch;
         o.adjoint = adjoint;

@@ -32,8 +32,7 @@
 namespace lbm {
 
 constexpr int kTickBlock = kFixBlock;  // fix-up items use the CTA as it is
-constexpr int kErrSpinTimeout = 4;
-constexpr long long kSpinLimit = 1LL << 22;  // polls of >= 128 ns: about a second
+constexpr long long kSpinLimit = 1LL << 22;  // polls of >= 128 ns: about a second (the largest limit)
 
 struct TickItems {
     const int4* amap;  // {replica, kind (0 static tile, 1 particle slot), tile or particle, dy | dz << 16}
@@ -42,7 +41,9 @@ struct TickItems {
     const int2* dmap;  // {replica, tile}
     long long na, nb, nc, nd;
     int d_test;  // 1: D items skip tiles near boundary work (A covers them); 0: D is every tile
-    int pad;
+    int wait_extra;        // added to the target of the B items' wait: 0, except in a test that makes
+                           // that wait run out (a target no count reaches)
+    long long spin_limit;  // polls before a wait gives up, in [1, kSpinLimit]
 };
 
 struct TickCounters {
@@ -58,12 +59,13 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     return v;
 }
 
-// the CTA waits (thread 0 polls, bounded) until *ctr >= target
-__device__ __forceinline__ void cta_wait(const int* ctr, int target, int* err) {
+// the CTA waits (thread 0 polls, at most `limit` times) until *ctr >= target
+__device__ __forceinline__ void cta_wait(const int* ctr, int target, int* err, long long limit) {
     if (threadIdx.x == 0) {
         long long it = 0;
+        if (limit < 1 || limit > kSpinLimit) limit = kSpinLimit;
         while (ld_acquire_gpu(ctr) < target) {
-            if (++it > kSpinLimit) {
+            if (++it > limit) {
                 atomicOr(err, kErrSpinTimeout);
                 break;
             }
@@ -146,12 +148,12 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
             if (tile >= 0) bulk_v4_tile<L, ST, TRT, B>(A, tile, s_ex);
             cta_done(&q->cnt_a);
         } else if (t < nab) {
-            cta_wait(&q->cnt_a, (int)it.na, err);
+            cta_wait(&q->cnt_a, (int)it.na + it.wait_extra, err, it.spin_limit);
             const int2 m = it.bmap[t - it.na];
             fixup_body<L, ST, TRT, kTickBlock>(args[m.x], m.y);
             cta_done(&q->cnt_b);
         } else if (t < nabc) {
-            cta_wait(&q->cnt_b, (int)it.nb, err);
+            cta_wait(&q->cnt_b, (int)it.nb, err, it.spin_limit);
             const int2 m = it.cmap[t - nab];
             particles_body<L, 128>(pargs[m.x], m.y);
         } else {

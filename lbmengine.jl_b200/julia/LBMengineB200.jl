@@ -23,7 +23,7 @@ struct LbmConfig
     force::NTuple{3,Float64}; force_field::Ptr{Float64}; wall_mask::Ptr{UInt8}
     wall_velocity::Ptr{Float64}; rho_init::Ptr{Float64}; u_init::Ptr{Float64}
     rho_uniform::Float64; u_uniform::NTuple{3,Float64}; rho_ref::Float64; store_scale::Float64
-    device::Int32; schedule::Int32
+    device::Int32; schedule::Int32; particle_rules::Int32; reserved::Int32
 end
 
 struct LbmParticleParams
@@ -38,6 +38,13 @@ struct LbmParticleState
     radius::Float64; inverse_mass::Float64; inverse_inertia::Float64; B1::Float64; B2::Float64
     position::NTuple{3,Float64}; velocity::NTuple{3,Float64}; angular_velocity::NTuple{3,Float64}
     swimming_direction::NTuple{3,Float64}; last_force::NTuple{3,Float64}; last_torque::NTuple{3,Float64}
+end
+
+struct LbmInfo
+    dims::Int32; lattice::Int32; q::Int32; storage::Int32
+    n::NTuple{3,Int64}; cells::Int64; tick::Int64; time::Float64
+    num_particles::Int32; bytes_per_population::Int32; device_bytes::Int64
+    bulk_kernel::Int32; bulk_threads::Int32; bulk_stages::Int32; reserved::Int32
 end
 
 lastError(h::Ptr{Cvoid}) = unsafe_string(ccall((:lbm_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
@@ -74,7 +81,8 @@ function modelInit(; massDensity = :default, fluidVelocity = :default, velocitie
                    timeStep = :default, latticeParameter = :default, kineticParameter = 0.25,
                    xlims = :default, ylims = :default, zlims = :default, dims = 2,
                    walledDimensions = :default, walls = :default, movingWalls = :default,
-                   isFluidCompressible = true, forceDensity = :default, storage = :f32, device = -1)
+                   isFluidCompressible = true, forceDensity = :default, storage = :f32, device = -1,
+                   particleRules = :gpu)
     @assert any(x -> x == :default, [timeStep, relaxationTimeRatio, viscosity]) "timeStep, relaxationTimeRatio, and viscosity cannot be all simultaneously defined!"
     @assert any(x -> x == :default, [timeStep, latticeParameter]) "timeStep, and latticeParameter cannot be both simultaneously defined!"
     latticeParameter != :default && (timeStep = latticeParameter)
@@ -149,7 +157,8 @@ function modelInit(; massDensity = :default, fluidVelocity = :default, velocitie
                     ntuple(a -> a <= dims ? axes[a][1] : 0.0, 3), dt, tau, tau_minus,
                     collisionModel == :bgk ? 0 : 1, isFluidCompressible ? 1 : 0, fmode, store, fvec,
                     ffield === nothing ? C_NULL : pointer(ffield), wall === nothing ? C_NULL : pointer(wall),
-                    uw === nothing ? C_NULL : pointer(uw), rho_ptr, u_ptr, rho_u, u_u, 0.0, 0.0, device, 0)
+                    uw === nothing ? C_NULL : pointer(uw), rho_ptr, u_ptr, rho_u, u_u, 0.0, 0.0, device, 0,
+                    particleRules == :cpu ? 1 : 0, 0)
     h = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve keep check(ccall((:lbm_create, LIB), Cint, (Ref{LbmConfig}, Ref{Ptr{Cvoid}}), cfg, h))
     schemes = Symbol[collisionModel]
@@ -254,9 +263,10 @@ function Base.getproperty(m::LBMmodel, s::Symbol)
                                     inverseMass = p.inverse_mass, inverseMomentOfInertia = p.inverse_inertia))
                 for p in st]
     elseif s === :tick || s === :time
-        info = Vector{UInt8}(undef, 128)
-        check(ccall((:lbm_get_info, LIB), Cint, (Ptr{Cvoid}, Ptr{UInt8}), getfield(m, :handle), info), getfield(m, :handle))
-        return s === :tick ? reinterpret(Int64, info[49:56])[1] : reinterpret(Float64, info[57:64])[1]
+        info = Ref{LbmInfo}()
+        check(ccall((:lbm_get_info, LIB), Cint, (Ptr{Cvoid}, Ref{LbmInfo}), getfield(m, :handle), info),
+              getfield(m, :handle))
+        return s === :tick ? info[].tick : info[].time
     end
     return getfield(m, s)
 end

@@ -28,6 +28,9 @@ LBM_FORCE_NONE, LBM_FORCE_UNIFORM, LBM_FORCE_FIELD = 0, 1, 2
 STORAGE_NAMES = {"f32": LBM_STORE_F32, "f16": LBM_STORE_F16, "bf16": LBM_STORE_BF16, "f64": LBM_STORE_F64}
 LBM_SCHEDULE_AUTO, LBM_SCHEDULE_STREAM, LBM_SCHEDULE_PERSISTENT = 0, 1, 3
 SCHEDULE_NAMES = {"auto": LBM_SCHEDULE_AUTO, "stream": LBM_SCHEDULE_STREAM, "persistent": LBM_SCHEDULE_PERSISTENT}
+LBM_RULES_GPU_MODULE, LBM_RULES_CPU_MODULE = 0, 1
+LBM_BULK_AUTO, LBM_BULK_VECTOR, LBM_BULK_TMA, LBM_BULK_SCALAR = 0, 1, 2, 3
+RULES_NAMES = {"gpu": LBM_RULES_GPU_MODULE, "cpu": LBM_RULES_CPU_MODULE}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -59,6 +62,8 @@ class LbmConfig(C.Structure):
         ("store_scale", C.c_double),
         ("device", C.c_int32),
         ("schedule", C.c_int32),
+        ("particle_rules", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -112,6 +117,10 @@ class LbmInfo(C.Structure):
         ("num_particles", C.c_int32),
         ("bytes_per_population", C.c_int32),
         ("device_bytes", C.c_int64),
+        ("bulk_kernel", C.c_int32),
+        ("bulk_threads", C.c_int32),
+        ("bulk_stages", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -189,6 +198,9 @@ PROTOTYPES = [
     ("lbm_save_state", C.c_int, [C.c_void_p, C.c_char_p]),
     ("lbm_load_state", C.c_int, [C.c_void_p, C.c_char_p]),
     ("lbm_step_noalloc", C.c_int, [C.c_void_p, C.c_int64]),
+    ("lbm_set_wait_limit", C.c_int, [C.c_void_p, C.c_int64, C.c_int32]),
+    ("lbm_set_memory_limit", C.c_int, [C.c_int64]),
+    ("lbm_set_bulk_kernel", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_last_global_error", C.c_char_p, []),
     ("lbm_destroy", None, [C.c_void_p]),
@@ -204,6 +216,7 @@ PROTOTYPES = [
     ("lbm_batch_get_tuning", C.c_int, [C.c_void_p, C.POINTER(LbmBatchTuning)]),
     ("lbm_batch_set_profiling", C.c_int, [C.c_void_p, C.c_int32]),
     ("lbm_batch_get_profile", C.c_int, [C.c_void_p, C.POINTER(LbmProfile)]),
+    ("lbm_batch_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_batch_destroy", None, [C.c_void_p]),
 ]

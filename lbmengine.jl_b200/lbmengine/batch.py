@@ -64,6 +64,12 @@ class LBMbatch:
         """Advance every replica by n ticks."""
         self._check(self._lib.lbm_batch_step(self._b, int(n)))
 
+    def status(self):
+        """Per replica: LBM_OK, or LBM_ERR_NUMERIC once its density went non-finite or negative."""
+        st = (C.c_int32 * len(self))()
+        self._lib.lbm_batch_status(self._b, st)
+        return list(st)
+
     def autotune(self, ticks: int = 16):
         """Time every tuning candidate and keep the fastest: (chosen, [candidates])."""
         cap = 64

@@ -101,7 +101,8 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
                   kineticParameter=0.25, xlims=DEFAULT, ylims=DEFAULT, zlims=DEFAULT, dims=2,
                   walledDimensions=DEFAULT, dampenEcho=False, walls=DEFAULT, movingWalls=DEFAULT,
                   isFluidCompressible=True, forceDensity=DEFAULT, forcingScheme=DEFAULT, saveData=False,
-                  storage="f32", rho_ref=DEFAULT, store_scale=DEFAULT, device=DEFAULT, schedule="auto"):
+                  storage="f32", rho_ref=DEFAULT, store_scale=DEFAULT, device=DEFAULT, schedule="auto",
+                  particleRules="gpu"):
     """Resolve modelInit's keywords (src/gpu/initMethods.jl:440-702) into an LbmConfig.
 
     Returns a namespace with ``cfg`` (capi.LbmConfig), ``keep`` (arrays the
@@ -247,6 +248,11 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
     if schedule not in capi.SCHEDULE_NAMES:
         raise ValueError(f"schedule must be one of {sorted(capi.SCHEDULE_NAMES)}")
     cfg.schedule = capi.SCHEDULE_NAMES[schedule]
+    # particleRules: "gpu" follows moveParticles! of src/gpu/particles.jl:7-92 (the module the
+    # reference loads when CUDA is functional), "cpu" that of src/cpu/particles.jl:48-100
+    if particleRules not in capi.RULES_NAMES:
+        raise ValueError(f"particleRules must be one of {sorted(capi.RULES_NAMES)}")
+    cfg.particle_rules = capi.RULES_NAMES[particleRules]
     return SimpleNamespace(cfg=cfg, keep=keep, dt=dt, tau=tau, tau_minus=tau_minus, viscosity=nu,
                            relaxationTimeRatio=ratio, coordinates=axes, shape=shape, dims=dims,
                            velocities=vname, collision=cm, schemes=list(dict.fromkeys(schemes)),

@@ -26,6 +26,10 @@
  *   getNodeVelocity           src/gpu/aux.jl:229-263, kernels src/gpu/kernels.jl:376-415
  *   moveParticles!            src/gpu/particles.jl:7-92
  *   cross (2D/3D)             src/gpu/aux.jl:139-157
+ * CPU-module particle rules (lbm_config.particle_rules == LBM_RULES_CPU_MODULE):
+ *   moveParticles! / eulerStep!  src/cpu/particles.jl:7-18, :48-100
+ *   bulkVelocity              src/cpu/particles.jl:21-46, cross src/cpu/aux.jl:19-28
+ *   Ladd momentum inputs      src/cpu/fluids.jl:423-438 (per-direction inputs, summed)
  * Floating-point operations are written in the reference's evaluation order
  * (left to right, no fused multiply-add: build with -ffp-contract=off).
  * Reductions the reference does with CUDA.jl parallel sums are done here
@@ -138,6 +142,10 @@ struct Particle {
     Real F[3] = {0, 0, 0}, T[3] = {0, 0, 0};  // forceInput / torqueInput
     Real lastF[3] = {0, 0, 0}, lastT[3] = {0, 0, 0};
     std::vector<uint8_t> S;  // solidRegion
+    std::vector<int64_t> solid;  // cells with S set, ascending
+    // CPU-module rules: momentumInput / angularMomentumInput, one slot per
+    // streaming direction (src/cpu/fluids.jl:434-437), summed at the move
+    std::vector<std::array<Real, 3>> dP, dL;
     // state captured by the last getNodeVelocity call (nodeVelocity is a
     // function of it, evaluated on demand)
     Real nvR[3] = {0, 0, 0}, nvV[3] = {0, 0, 0}, nvW[3] = {0, 0, 0}, nvE[3] = {0, 0, 0};
@@ -161,6 +169,22 @@ struct Model {
     std::vector<Particle<Real>> parts;
     int64_t tick = 0;
     double time = 0;
+    int rules = LBM_RULES_GPU_MODULE;
+    // bit id of wmark[c]: c is fluid and c - c_id a wall node (the walls'
+    // streamingInvasionRegions of the opposite direction); mark[c] adds the
+    // particles' regions for the current tick
+    std::vector<uint32_t> wmark, mark;
+    // wrapped index of i + s along axis a: wrap[a][s + 1][i], s in {-1, 0, 1}
+    std::vector<int64_t> wrap[3][3];
+
+    void build_wrap() {
+        for (int a = 0; a < 3; ++a)
+            for (int s = -1; s <= 1; ++s) {
+                auto& t = wrap[a][s + 1];
+                t.resize(n[a]);
+                for (int64_t i = 0; i < n[a]; ++i) t[i] = ((i + s) % n[a] + n[a]) % n[a];
+            }
+    }
 
     int64_t cell(int64_t x, int64_t y, int64_t z) const { return x + n[0] * (y + n[1] * z); }
     void coords(int64_t c, int64_t& x, int64_t& y, int64_t& z) const {
@@ -216,8 +240,10 @@ void axis_range(const Model<Real>& m, int a, double Ra, double r2, int64_t& lo, 
 }
 
 template <class Real>
-void get_sphere(const Model<Real>& m, double radius, const Real* R, std::vector<uint8_t>& S) {
+void get_sphere(const Model<Real>& m, double radius, const Real* R, std::vector<uint8_t>& S,
+                std::vector<int64_t>* solid = nullptr) {
     S.assign(m.N, 0);
+    if (solid) solid->clear();
     double r2 = radius * radius;
     int64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     for (int a = 0; a < m.dims; ++a) axis_range(m, a, val(R[a]), r2, lo[a], hi[a]);
@@ -225,7 +251,10 @@ void get_sphere(const Model<Real>& m, double radius, const Real* R, std::vector<
     for (int64_t z = lo[2]; z <= hi[2]; ++z)
         for (int64_t y = lo[1]; y <= hi[1]; ++y)
             for (int64_t x = lo[0]; x <= hi[0]; ++x)
-                if (in_sphere(m, x, y, z, R, r2)) S[m.cell(x, y, z)] = 1;
+                if (in_sphere(m, x, y, z, R, r2)) {
+                    S[m.cell(x, y, z)] = 1;
+                    if (solid) solid->push_back(m.cell(x, y, z));
+                }
 }
 
 // dot of a vector with a lattice vector, vectorFieldDotVector (kernels.jl:198-224):
@@ -305,79 +334,113 @@ void hydro(Model<Real>& m) {
     }
 }
 
-// equilibriumDistribution (fluids.jl:39-52) at one cell
+// Relaxation and Guo prefactors of one tick.  The reference evaluates them
+// inside its per-node expressions; each is the same rounded value at every
+// node, so computing it once gives the same results.
 template <class Real>
-inline Real feq(const Model<Real>& m, int i, int64_t c) {
-    const int d = m.dims;
-    Real uc = 0.0, uu = 0.0;
-    for (int k = 0; k < d; ++k) uc += m.u[(int64_t)k * m.N + c] * (double)m.vs.c[i][k];
-    for (int k = 0; k < d; ++k) uu += m.u[(int64_t)k * m.N + c] * m.u[(int64_t)k * m.N + c];
-    Real first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
-    Real second = first - uu * (0.5 * m.invC2);
-    double wi = m.vs.w[i];
-    if (m.compressible) return wi * ((second + 1) * m.rho[c]);
-    return wi * m.rho[c] + wi * (m.rho0[c] * second);
+struct CollideConsts {
+    Real om, om_p, om_m;      // -dt/tau, -dt/tau+, -dt/tau-
+    Real kb, kp, km;          // 1 - dt/(2 tau), 1 - dt/(2 tau+), 1 - dt/(2 tau-)
+};
+
+template <class Real>
+CollideConsts<Real> collide_consts(const Model<Real>& m) {
+    CollideConsts<Real> k;
+    k.om = -m.dt / m.tau;
+    k.om_p = -m.dt / m.tau_plus;
+    k.om_m = -m.dt / m.tau_minus;
+    k.kb = 1 - m.dt / (2 * m.tau);
+    k.kp = 1 - m.dt / (2 * m.tau_plus);
+    k.km = 1 - m.dt / (2 * m.tau_minus);
+    return k;
 }
 
-// guoForcingTerm (fluids.jl:103-127) at one cell
+// collisionStep (fluids.jl:58-101) with equilibriumDistribution (:39-52) and
+// guoForcingTerm (:103-127) at one cell: fs_i = f_i + Omega_i (+ G_i).
+// Per direction, with uc = u.c_i and uu = u.u (sums from 0 in component order):
+//   f_eq = w ((uc/cs2 + uc^2/(2 cs4) - uu/(2 cs2) + 1) rho)            compressible
+//        = w rho + w (rho0 (uc/cs2 + uc^2/(2 cs4) - uu/(2 cs2)))       incompressible
+//   BGK  Omega = (-dt/tau)(f - f_eq),
+//        G = w dt (1 - dt/2tau) sum_k ((c_k - u_k)/cs2 + uc c_k/cs4) F_k
+//   TRT  Omega = (-dt/tau+)(f+ - f_eq+) + (-dt/tau-)(f- - f_eq-),
+//        G = w dt ((1 - dt/2tau+) sum_k (-u_k/cs2 + uc c_k/cs4) F_k
+//                 + (1 - dt/2tau-) sum_k F_k c_k/cs2)
+// The products u.c_i and u.u are the same values in the equilibrium and in
+// the Guo term; each is computed once per cell.
 template <class Real>
-inline Real guo(const Model<Real>& m, int i, int64_t c) {
-    const int d = m.dims;
-    const auto& ci = m.vs.c[i];
-    Real U[3] = {0, 0, 0}, Fv[3] = {0, 0, 0};
-    for (int k = 0; k < d; ++k) {
-        U[k] = m.u[(int64_t)k * m.N + c];
-        Fv[k] = m.F[(int64_t)k * m.N + c];
+inline void collide_cell(const Model<Real>& m, const CollideConsts<Real>& K, int64_t c, Real* out) {
+    const int64_t N = m.N;
+    const int d = m.dims, Q = m.vs.q;
+    Real U[3] = {0, 0, 0}, Fv[3] = {0, 0, 0}, f[27], eq[27], uc[27];
+    for (int k = 0; k < d; ++k) U[k] = m.u[(int64_t)k * N + c];
+    if (m.guo)
+        for (int k = 0; k < d; ++k) Fv[k] = m.F[(int64_t)k * N + c];
+    Real uu = 0.0;
+    for (int k = 0; k < d; ++k) uu += U[k] * U[k];
+    const Real rho = m.rho[c];
+    for (int i = 0; i < Q; ++i) {
+        f[i] = m.f[(int64_t)i * N + c];
+        Real x = 0.0;
+        for (int k = 0; k < d; ++k) x += U[k] * (double)m.vs.c[i][k];
+        uc[i] = x;
+        Real first = x * m.invC2 + (x * x) * (0.5 * m.invC4);
+        Real second = first - uu * (0.5 * m.invC2);
+        const double wi = m.vs.w[i];
+        eq[i] = m.compressible ? wi * ((second + 1) * rho) : wi * rho + wi * (m.rho0[c] * second);
     }
-    Real uc = 0.0;
-    for (int k = 0; k < d; ++k) uc += U[k] * (double)ci[k];
-    double wi = m.vs.w[i];
-    if (!m.trt) {
-        Real inter = 0.0;
-        for (int k = 0; k < d; ++k) {
-            Real second = (uc * (double)ci[k]) * m.invC4;
-            Real first = ((-U[k]) + (double)ci[k]) * m.invC2;
-            inter += (first + second) * Fv[k];
+    for (int i = 0; i < Q; ++i) {
+        const Real fi = f[i];
+        Real om;
+        if (!m.trt) {
+            om = K.om * (fi - eq[i]);
+        } else {
+            const int ib = m.vs.opp[i];
+            const Real fb = f[ib];
+            Real fp = 0.5 * (fi + fb), fm = 0.5 * (fi - fb);
+            Real ep = 0.5 * (eq[i] + eq[ib]), em = 0.5 * (eq[i] - eq[ib]);
+            om = K.om_p * (fp - ep) + K.om_m * (fm - em);
         }
-        return wi * m.dt * (1 - m.dt / (2 * m.tau)) * inter;
+        if (m.guo) {
+            const auto& ci = m.vs.c[i];
+            const double wi = m.vs.w[i];
+            Real G;
+            if (!m.trt) {
+                Real inter = 0.0;
+                for (int k = 0; k < d; ++k) {
+                    Real second = (uc[i] * (double)ci[k]) * m.invC4;
+                    Real first = ((-U[k]) + (double)ci[k]) * m.invC2;
+                    inter += (first + second) * Fv[k];
+                }
+                G = wi * m.dt * K.kb * inter;
+            } else {
+                Real inter = 0.0;
+                for (int k = 0; k < d; ++k) {
+                    Real second = (uc[i] * (double)ci[k]) * m.invC4;
+                    inter += ((-U[k]) * m.invC2 + second) * Fv[k];
+                }
+                Real plus = K.kp * inter;
+                Real inter2 = 0.0;
+                for (int k = 0; k < d; ++k) inter2 += Fv[k] * ((double)ci[k] * m.invC2);
+                Real minus = K.km * inter2;
+                G = wi * m.dt * (plus + minus);
+            }
+            om = om + G;
+        }
+        out[i] = om + fi;
     }
-    Real inter = 0.0;
-    for (int k = 0; k < d; ++k) {
-        Real second = (uc * (double)ci[k]) * m.invC4;
-        inter += ((-U[k]) * m.invC2 + second) * Fv[k];
-    }
-    Real plus = (1 - m.dt / (2 * m.tau_plus)) * inter;
-    Real inter2 = 0.0;
-    for (int k = 0; k < d; ++k) inter2 += Fv[k] * ((double)ci[k] * m.invC2);
-    Real minus = (1 - m.dt / (2 * m.tau_minus)) * inter2;
-    return wi * m.dt * (plus + minus);
 }
 
-// collisionStep (fluids.jl:58-101): returns f + Omega
 template <class Real>
 void collision(const Model<Real>& m, std::vector<Real>& fs) {
     const int64_t N = m.N;
     const int Q = m.vs.q;
+    const CollideConsts<Real> K = collide_consts(m);
     fs.resize((size_t)N * Q);
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < N; ++c) {
-        Real eq[27];
-        for (int i = 0; i < Q; ++i) eq[i] = feq(m, i, c);
-        for (int i = 0; i < Q; ++i) {
-            Real fi = m.f[(int64_t)i * N + c];
-            Real om;
-            if (!m.trt) {
-                om = (-m.dt / m.tau) * (fi - eq[i]);
-            } else {
-                int ib = m.vs.opp[i];
-                Real fb = m.f[(int64_t)ib * N + c];
-                Real fp = 0.5 * (fi + fb), fm = 0.5 * (fi - fb);
-                Real ep = 0.5 * (eq[i] + eq[ib]), em = 0.5 * (eq[i] - eq[ib]);
-                om = (-m.dt / m.tau_plus) * (fp - ep) + (-m.dt / m.tau_minus) * (fm - em);
-            }
-            if (m.guo) om = om + guo(m, i, c);
-            fs[(int64_t)i * N + c] = om + fi;
-        }
+        Real out[27];
+        collide_cell(m, K, c, out);
+        for (int i = 0; i < Q; ++i) fs[(int64_t)i * N + c] = out[i];
     }
 }
 
@@ -401,18 +464,72 @@ void cross_ref(int d, const A* v, const B* w, C* out) {
     }
 }
 
-// sorted fluid cells x with x - c_id in S and x not in S (conjugate boundary nodes)
+// sorted fluid cells x with x - c_id in S and x not in S (conjugate boundary nodes),
+// from the particle's solid cells (the same set as a scan of the whole grid)
 template <class Real>
 void particle_links(const Model<Real>& m, const Particle<Real>& p, int id, std::vector<int64_t>& out) {
     out.clear();
     const auto& ci = m.vs.c[id];
     if (ci[0] == 0 && ci[1] == 0 && ci[2] == 0) return;
-    for (int64_t y = 0; y < m.N; ++y) {
-        if (!p.S[y]) continue;
-        int64_t x = m.shifted(y, ci[0], ci[1], ci[2]);
+    for (int64_t y : p.solid) {
+        const int64_t x = m.shifted(y, ci[0], ci[1], ci[2]);
         if (!p.S[x]) out.push_back(x);
     }
     std::sort(out.begin(), out.end());
+}
+
+// bulkVelocity of the CPU module at node y (src/cpu/particles.jl:21-46), with
+// the state captured at the last node-velocity update: v + cross(w, x - R)
+// (cross of src/cpu/aux.jl:19-28; in 2D the scalar w acts as (0, 0, w)), plus
+// the squirmer slip (B1 + B2 e.r)((e.r) r - e) with r = (x - R)/|x - R|.
+// `norm` is LinearAlgebra's generic 2-norm (0 for a zero vector); `dot` is
+// summed in component order.  Nodes farther than 2 dx from the surface get
+// zero (:25), which no boundary link reaches: a solid node next to a fluid
+// node lies within sqrt(d) dx of the surface.
+template <class Real>
+void node_velocity_cpu(const Model<Real>& m, const Particle<Real>& p, int64_t y, Real* out) {
+    const int d = m.dims;
+    Real xr[3] = {0, 0, 0};
+    for (int k = 0; k < d; ++k) xr[k] = m.coord(k, y) - p.nvR[k];
+    double mx = 0.0;
+    for (int k = 0; k < d; ++k) mx = std::max(mx, std::fabs(val(xr[k])));
+    Real nrm = 0.0;
+    if (mx != 0.0) {
+        Real s2 = xr[0] * xr[0];
+        for (int k = 1; k < d; ++k) s2 += xr[k] * xr[k];
+        nrm = sqrt(s2);
+    }
+    if (std::fabs(val(nrm) - p.radius) > 2 * m.dx) {
+        for (int k = 0; k < d; ++k) out[k] = 0.0;
+        return;
+    }
+    Real bulk[3];
+    if (d == 2) {
+        Real c0 = 0.0 * 0.0 - p.nvW[0] * xr[1];
+        Real c1 = (-0.0) * 0.0 + p.nvW[0] * xr[0];
+        bulk[0] = p.nvV[0] + c0;
+        bulk[1] = p.nvV[1] + c1;
+    } else {
+        Real c0 = p.nvW[1] * xr[2] - p.nvW[2] * xr[1];
+        Real c1 = (-p.nvW[0]) * xr[2] + p.nvW[2] * xr[0];
+        Real c2 = p.nvW[0] * xr[1] - p.nvW[1] * xr[0];
+        bulk[0] = p.nvV[0] + c0;
+        bulk[1] = p.nvV[1] + c1;
+        bulk[2] = p.nvV[2] + c2;
+    }
+    if (p.kind == LBM_BEAD || nrm == 0.0) {
+        for (int k = 0; k < d; ++k) out[k] = bulk[k];
+        return;
+    }
+    Real fr[3];
+    for (int k = 0; k < d; ++k) fr[k] = xr[k] / nrm;
+    Real edr = p.nvE[0] * fr[0];
+    for (int k = 1; k < d; ++k) edr += p.nvE[k] * fr[k];
+    Real first = p.B1 + p.B2 * edr;
+    for (int k = 0; k < d; ++k) {
+        Real second = edr * fr[k] - p.nvE[k];
+        out[k] = first * second + bulk[k];
+    }
 }
 
 // moveParticles! (particles.jl:7-92)
@@ -483,17 +600,88 @@ void move_particle(Model<Real>& m, Particle<Real>& p, bool initial) {
         p.F[k] = 0;
         p.T[k] = 0;
     }
-    if (moved) get_sphere(m, p.radius, p.R, p.S);
+    if (moved) get_sphere(m, p.radius, p.R, p.S, &p.solid);
     if (need_nv) capture_node_velocity(p);
+}
+
+// moveParticles! of the CPU module (src/cpu/particles.jl:48-100): the inputs
+// of all directions summed in direction order, v += m^-1 dP, w += I^-1 dL, an
+// Euler step R += dt v whenever v != 0 (eulerStep!, :7-18: spherical
+// particles never rotate), node velocities refreshed when dL != 0 or the
+// particle moved.  last force/torque report dP and dL.
+template <class Real>
+void move_particle_cpu(Model<Real>& m, Particle<Real>& p, bool initial) {
+    const int d = m.dims, nw = d == 2 ? 1 : 3, Q = m.vs.q;
+    bool moved = initial, need_nv = initial;
+    Real dP[3] = {0, 0, 0}, dL[3] = {0, 0, 0};
+    if (!p.dP.empty()) {
+        for (int k = 0; k < 3; ++k) {
+            dP[k] = p.dP[0][k] + p.dP[1][k];
+            dL[k] = p.dL[0][k] + p.dL[1][k];
+            for (int id = 2; id < Q; ++id) {
+                dP[k] += p.dP[id][k];
+                dL[k] += p.dL[id][k];
+            }
+        }
+    }
+    if (!initial) {
+        for (int k = 0; k < d; ++k) p.v[k] = p.v[k] + p.inv_mass * dP[k];
+        for (int k = 0; k < nw; ++k) p.w[k] = p.w[k] + p.inv_inertia * dL[k];
+        bool vnz = false;
+        for (int k = 0; k < d; ++k) vnz = vnz || (p.v[k] != 0.0);
+        if (vnz) {
+            for (int k = 0; k < d; ++k) p.R[k] = p.R[k] + m.dt * p.v[k];
+            moved = true;
+        }
+        for (int k = 0; k < nw; ++k)
+            if (dL[k] != 0.0) need_nv = true;
+        need_nv = need_nv || moved;
+    }
+    for (int k = 0; k < 3; ++k) {
+        p.lastF[k] = dP[k];
+        p.lastT[k] = dL[k];
+        p.F[k] = 0;
+        p.T[k] = 0;
+    }
+    p.dP.assign(Q, {Real(0.0), Real(0.0), Real(0.0)});
+    p.dL.assign(Q, {Real(0.0), Real(0.0), Real(0.0)});
+    if (moved) get_sphere(m, p.radius, p.R, p.S, &p.solid);
+    if (need_nv) capture_node_velocity(p);
+}
+
+template <class Real>
+void move(Model<Real>& m, Particle<Real>& p, bool initial) {
+    if (m.rules == LBM_RULES_CPU_MODULE) move_particle_cpu(m, p, initial);
+    else move_particle(m, p, initial);
+}
+
+// marks of the current tick: the walls' (static) plus every particle's
+// streamingInvasionRegions; bit id of mark[c] set when f_id(c) takes the
+// bounce-back value (c fluid for that solid, c - c_id solid)
+template <class Real>
+void build_marks(Model<Real>& m) {
+    m.mark = m.wmark;
+    if (!m.ladd) return;
+    const int Q = m.vs.q;
+    for (const auto& p : m.parts)
+        for (int64_t y : p.solid)
+            for (int id = 1; id < Q; ++id) {
+                const auto& ci = m.vs.c[id];
+                const int64_t x = m.shifted(y, ci[0], ci[1], ci[2]);
+                if (!p.S[x]) m.mark[x] |= 1u << id;
+            }
 }
 
 template <class Real>
 void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
     const int64_t N = m.N;
     const int Q = m.vs.q, d = m.dims;
+    const int64_t n0 = m.n[0], n1 = m.n[1], rows = m.n[1] * m.n[2];
+    const bool cpu = m.rules == LBM_RULES_CPU_MODULE;
     collision(m, fs);
     fn.resize((size_t)N * Q);
     const double coeff = std::pow(m.dx, d) / m.dt;
+    if (m.bounce_back) build_marks(m);
     std::vector<int64_t> nodes;
     for (int id = 0; id < Q; ++id) {
         const auto& ci = m.vs.c[id];
@@ -502,26 +690,32 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
         Real* s = &fn[(size_t)id * N];
         const Real* fsi = &fs[(size_t)id * N];
         const Real* fsb = &fs[(size_t)ib * N];
+        const int64_t* wx = m.wrap[0][1 - ci[0]].data();
+        const int64_t* wy = m.wrap[1][1 - ci[1]].data();
+        const int64_t* wz = m.wrap[2][1 - ci[2]].data();
+        const uint32_t bit = 1u << id;
 #pragma omp parallel for schedule(static)
-        for (int64_t c = 0; c < N; ++c) {
-            // circshift (pull): out(x) = in(x - c)
-            Real v = fsi[m.shifted(c, -ci[0], -ci[1], -ci[2])];
-            if (m.bounce_back) {
-                if (m.W[c]) v = 0;
-                bool region = invasion(m, m.W, ib, c);
-                if (m.ladd)
-                    for (const auto& p : m.parts) region = region || invasion(m, p.S, ib, c);
-                if (region) {
-                    v = fsb[c];
-                    if (m.moving_walls) {
-                        int64_t src = m.shifted(c, -ci[0], -ci[1], -ci[2]);
-                        double uwv[3];
-                        for (int k = 0; k < d; ++k) uwv[k] = m.uw[(int64_t)k * N + src];
-                        v += (2 * wi * m.invC2) * m.rho[c] * dot_c(uwv, ci, d);
+        for (int64_t row = 0; row < rows; ++row) {
+            const int64_t y = row % n1, z = row / n1;
+            const int64_t srow = n0 * (wy[y] + n1 * wz[z]);
+            for (int64_t x = 0; x < n0; ++x) {
+                const int64_t c = x + n0 * row;
+                const int64_t src = wx[x] + srow;
+                // circshift (pull): out(x) = in(x - c)
+                Real v = fsi[src];
+                if (m.bounce_back) {
+                    if (m.W[c]) v = 0;
+                    if (m.mark[c] & bit) {  // streaming invasion exchange (walls and particles)
+                        v = fsb[c];
+                        if (m.moving_walls) {
+                            double uwv[3];
+                            for (int k = 0; k < d; ++k) uwv[k] = m.uw[(int64_t)k * N + src];
+                            v += (2 * wi * m.invC2) * m.rho[c] * dot_c(uwv, ci, d);
+                        }
                     }
                 }
+                s[c] = v;
             }
-            s[c] = v;
         }
         if (m.bounce_back && m.ladd) {
             for (auto& p : m.parts) {
@@ -530,14 +724,25 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
                 for (int64_t x : nodes) {
                     int64_t src = m.shifted(x, -ci[0], -ci[1], -ci[2]);
                     Real up[3];
-                    node_velocity(m, p, src, up);
+                    if (cpu) {
+                        // uw = u_p(x) + u_p(x - c) (src/cpu/fluids.jl:429); x is fluid, u_p(x) = 0
+                        node_velocity_cpu(m, p, src, up);
+                        for (int k = 0; k < d; ++k) up[k] = 0.0 + up[k];
+                    } else {
+                        node_velocity(m, p, src, up);
+                    }
                     s[x] += (2 * wi * m.invC2) * m.rho[x] * dot_c(up, ci, d);
                 }
                 if (p.couple_f || p.couple_t) {
                     if (p.couple_f) {
                         Real S = 0.0;
                         for (int64_t x : nodes) S += fsb[x] + s[x];
-                        for (int k = 0; k < d; ++k) p.F[k] -= coeff * S * (double)ci[k];
+                        if (cpu) {  // momentumInput[id] -= dx^d sum(sumTerm) c (dx/dt)
+                            const Real t = std::pow(m.dx, d) * S;
+                            for (int k = 0; k < d; ++k) p.dP[id][k] -= t * ((double)ci[k] * (m.dx / m.dt));
+                        } else {
+                            for (int k = 0; k < d; ++k) p.F[k] -= coeff * S * (double)ci[k];
+                        }
                     }
                     if (p.couple_t) {
                         Real aux[3] = {0, 0, 0};
@@ -547,9 +752,16 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
                         }
                         double cd[3] = {(double)ci[0], (double)ci[1], (double)ci[2]};
                         Real cr[3] = {0, 0, 0};
-                        cross_ref(d, aux, cd, cr);
                         int nt = d == 2 ? 1 : 3;
-                        for (int k = 0; k < nt; ++k) p.T[k] -= coeff * cr[k];
+                        if (cpu) {
+                            for (int k = 0; k < 3; ++k) cd[k] = cd[k] * (m.dx / m.dt);
+                            cross_ref(d, aux, cd, cr);
+                            const double ld = std::pow(m.dx, d);
+                            for (int k = 0; k < nt; ++k) p.dL[id][k] -= ld * cr[k];
+                        } else {
+                            cross_ref(d, aux, cd, cr);
+                            for (int k = 0; k < nt; ++k) p.T[k] -= coeff * cr[k];
+                        }
                     }
                 }
             }
@@ -560,7 +772,7 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
     m.tick += 1;
     hydro(m);
     if (m.ladd)
-        for (auto& p : m.parts) move_particle(m, p, false);
+        for (auto& p : m.parts) move(m, p, false);
 }
 
 template <class Real>
@@ -662,6 +874,15 @@ int create_model(const lbm_config* cfg, Model<Real>& m, const double* seed_tau_p
         return fail(LBM_ERR_INVALID, "unknown force mode");
     }
     m.rho0 = m.rho;
+    if (cfg->particle_rules != LBM_RULES_GPU_MODULE && cfg->particle_rules != LBM_RULES_CPU_MODULE)
+        return fail(LBM_ERR_INVALID, "unknown particle rules");
+    m.rules = cfg->particle_rules;
+    m.build_wrap();
+    m.wmark.assign(N, 0u);
+    if (m.bounce_back)
+        for (int64_t c = 0; c < N; ++c)
+            for (int id = 1; id < Q; ++id)
+                if (invasion(m, m.W, m.vs.opp[id], c)) m.wmark[c] |= 1u << id;
     // findInitialConditions (initMethods.jl:417-438)
     m.f.assign((size_t)N * Q, 0.0);
     for (int64_t c = 0; c < N; ++c) {
@@ -726,7 +947,7 @@ int add_particle(Model<Real>& m, const lbm_particle_params* pp, const double* se
     m.parts.push_back(p);
     m.ladd = true;
     m.bounce_back = true;  // addSquirmer!/addBead! install an empty wall if needed (:210-214)
-    move_particle(m, m.parts.back(), true);
+    move(m, m.parts.back(), true);
     if (id_out) *id_out = m.parts.back().id;
     return LBM_OK;
 }
@@ -824,6 +1045,26 @@ int orc_get_particles(void* hp, lbm_particle_state* out, int32_t cap, int32_t* c
             s.last_torque[k] = p.lastT[k];
         }
     }
+    return LBM_OK;
+}
+
+// Overwrite the position, velocity, angular velocity and swimming direction
+// of particle `id` (1-based) and re-voxelise it: its solid region and node
+// velocities are recomputed from the new state (the initial-setup branch of
+// moveParticles!, src/gpu/particles.jl:62-91), the momentum inputs are kept.
+int orc_set_particle(void* hp, int32_t id, const lbm_particle_state* st) {
+    if (!hp || !st) return fail(LBM_ERR_INVALID, "null argument");
+    Model<double>& m = static_cast<Handle*>(hp)->m;
+    if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
+    Particle<double>& p = m.parts[id - 1];
+    for (int k = 0; k < 3; ++k) {
+        p.R[k] = st->position[k];
+        p.v[k] = st->velocity[k];
+        p.w[k] = st->angular_velocity[k];
+        p.e[k] = st->swimming_direction[k];
+    }
+    get_sphere(m, p.radius, p.R, p.S, &p.solid);
+    capture_node_velocity(p);
     return LBM_OK;
 }
 

@@ -2,8 +2,10 @@
 
 Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg,
 always as the checker or the timed CPU baseline, never as a product path.
-The oracle restates LBMengine.jl's GPU-module time step in FP64; parity is
-unpinned by the reference itself (it ships no tests or golden vectors).
+The oracle restates LBMengine.jl's GPU-module time step in FP64, and with
+lbm_config.particle_rules == LBM_RULES_CPU_MODULE the CPU module's particle
+update; parity is unpinned by the reference itself (it ships no tests or
+golden vectors and its Julia toolchain is not available to run it).
 """
 from __future__ import annotations
 
@@ -57,6 +59,7 @@ def load() -> C.CDLL:
     lib.orc_set_distributions.argtypes = [vp, dp]
     lib.orc_get_particles.argtypes = [vp, C.POINTER(capi.LbmParticleState), C.c_int32, C.POINTER(C.c_int32)]
     lib.orc_get_mask.argtypes = [vp, C.c_int32, C.POINTER(C.c_uint8)]
+    lib.orc_set_particle.argtypes = [vp, C.c_int32, C.POINTER(capi.LbmParticleState)]
     lib.orc_get_links.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.c_int64,
                                   C.POINTER(C.c_int64)]
     lib.orc_get_info.argtypes = [vp, C.POINTER(capi.LbmInfo)]
@@ -144,6 +147,11 @@ class OracleModel:
         arr = (capi.LbmParticleState * max(1, cnt.value))()
         _check(self.lib.orc_get_particles(self.h, arr, cnt.value, C.byref(cnt)))
         return list(arr)[:cnt.value]
+
+    def set_particle(self, pid: int, state) -> None:
+        """Move particle `pid` to another state (position, velocity, angular velocity,
+        swimming direction of an LbmParticleState) and re-voxelise it there."""
+        _check(self.lib.orc_set_particle(self.h, pid, C.byref(state)))
 
     def mask(self, pid: int):
         m = np.zeros(self.cells, dtype=np.uint8)

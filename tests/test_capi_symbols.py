@@ -59,6 +59,8 @@ int main(void) {
   printf("%zu %zu %zu\n", sizeof(lbm_particle_state), offsetof(lbm_particle_state, last_torque),
          offsetof(lbm_particle_state, position));
   printf("%zu %zu\n", sizeof(lbm_info), offsetof(lbm_info, device_bytes));
+  printf("%zu %zu %zu %zu\n", offsetof(lbm_config, particle_rules), offsetof(lbm_info, tick),
+         offsetof(lbm_info, time), offsetof(lbm_info, bulk_kernel));
   printf("%zu %zu\n", sizeof(lbm_profile), offsetof(lbm_profile, profiled_steps));
   return 0;
 }
@@ -78,5 +80,36 @@ int main(void) {
            ctypes.sizeof(C.LbmParticleState), C.LbmParticleState.last_torque.offset,
            C.LbmParticleState.position.offset,
            ctypes.sizeof(C.LbmInfo), C.LbmInfo.device_bytes.offset,
+           C.LbmConfig.particle_rules.offset, C.LbmInfo.tick.offset, C.LbmInfo.time.offset,
+           C.LbmInfo.bulk_kernel.offset,
            ctypes.sizeof(C.LbmProfile), C.LbmProfile.profiled_steps.offset]
     assert got == exp
+
+
+def _c_fields(header, name):
+    """Field names of `typedef struct name {...} name;` in declaration order."""
+    m = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), header, flags=re.S)
+    body = re.sub(r"/\*.*?\*/", "", m.group(1), flags=re.S)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        m2 = re.search(r"(\w+)\s*(\[\s*\d+\s*\])?$", decl)
+        out.append(m2.group(1))
+    return out
+
+
+def _julia_fields(src, name):
+    m = re.search(r"struct %s\n(.*?)\nend" % name, src, flags=re.S)
+    return [f.split("::")[0].strip() for line in m.group(1).splitlines() for f in line.split(";") if "::" in f]
+
+
+def test_julia_struct_mirrors_follow_the_header():
+    """The Julia shim's ccall structs list the C fields in the header's order
+    (Julia is not installed here; this is a check of the source text)."""
+    header = open(os.path.join(REPO, "include", "lbm_b200.h")).read()
+    jl = open(os.path.join(REPO, "lbmengine.jl_b200", "julia", "LBMengineB200.jl")).read()
+    for c_name, j_name in (("lbm_config", "LbmConfig"), ("lbm_particle_params", "LbmParticleParams"),
+                           ("lbm_particle_state", "LbmParticleState"), ("lbm_info", "LbmInfo")):
+        assert _julia_fields(jl, j_name) == _c_fields(header, c_name), c_name
