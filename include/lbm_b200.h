@@ -101,8 +101,21 @@ typedef struct lbm_config {
     int32_t device;            /* CUDA device ordinal; < 0: the calling thread's current device */
     int32_t schedule;          /* LBM_SCHEDULE_*: how the kernels of a tick are launched */
     int32_t particle_rules;    /* LBM_RULES_*: which of the reference's two modules the particle update follows */
-    int32_t reserved;
+    int32_t rounding;          /* LBM_ROUND_*: rounding of the F16/BF16 stores */
 } lbm_config;
+
+/* Rounding of the populations stored in F16/BF16 (FP32/FP64 ignore it).
+ *   STOCHASTIC (default)  the fraction below the kept bits is rounded up when
+ *                         it exceeds a dither that is a hash of the cell and of
+ *                         kept bits of the node's values, so the rounding
+ *                         errors of a uniform region have zero mean instead
+ *                         of adding up tick after tick (a uniformly forced
+ *                         fluid otherwise drifts by ~1e-3 of its velocity
+ *                         within a few hundred ticks); deterministic, costs
+ *                         three integer operations per stored value
+ *   NEAREST               round to nearest even */
+#define LBM_ROUND_STOCHASTIC 0
+#define LBM_ROUND_NEAREST 1
 
 /* Particle update rules.  The reference has two implementations of the
  * particle update, picked when the package loads (src/LBMengine.jl:10-24):
@@ -225,6 +238,38 @@ int lbm_step(lbm_handle* h, int64_t nsteps);
  * tick (hydroVariablesUpdate!, src/gpu/fluids.jl:32-37).  Either may be NULL. */
 int lbm_get_fields(lbm_handle* h, double* rho, double* u);
 
+/* viscousStressTensor(model) (src/cpu/fluids.jl:507-520; the GPU module's
+ * copy is commented out, src/gpu/fluids.jl:272-285): sigma_ab =
+ * -(1 - dt/(2 tau)) sum_i c_ia c_ib (f_i - f_eq_i) at the current rho and u,
+ * as (N..., d, d) FP64 column-major, entry (a, b) of cell c at
+ * sigma[c + N*(a + d*b)], computed on the device. */
+int lbm_get_stress(lbm_handle* h, double* sigma);
+
+/* Output of LBMpropagate!(...) with the :saveData scheme (src/gpu/fluids.jl:243-259).
+ *
+ * lbm_record_trajectories: from now on the particle update records, after
+ * every tick, each particle's position, velocity and angular velocity
+ * (writeParticleTrajectory, src/gpu/aux.jl:319-356) into a device ring of
+ * `capacity` ticks (0: stop); no host synchronisation per tick, so stepping
+ * stays graph-replayed.  Adding a particle restarts the ring.
+ * lbm_read_trajectories: the ticks recorded since the last read, oldest
+ * first, as out[(t * P + p) * 9 + k] (k: position 0-2, velocity 3-5,
+ * angular velocity 6-8; 2D angular velocity at 6); *ticks = how many (with
+ * out == NULL only the count).  They are the last *ticks ticks of the model.
+ * LBM_ERR_STATE if more ticks than the ring holds passed since the last read.
+ *
+ * lbm_write_fluid_csv: writeTrajectories (src/gpu/aux.jl:271-317), the file
+ * `fluidTrj_<tick>.csv` of the reference: per node tick, time, id_*,
+ * coordinate_*, massDensity, fluidVelocity_*, f1..fQ, numbers printed as
+ * Julia prints them.  The fields are read back at once; the file is
+ * formatted and written by a host thread while the caller steps on.
+ * lbm_output_flush waits for it (and reports a failed write); the next
+ * lbm_write_fluid_csv and lbm_destroy wait too. */
+int lbm_record_trajectories(lbm_handle* h, int64_t capacity);
+int lbm_read_trajectories(lbm_handle* h, double* out, int64_t capacity, int64_t* ticks);
+int lbm_write_fluid_csv(lbm_handle* h, const char* path);
+int lbm_output_flush(lbm_handle* h);
+
 /* model.distributions (N..., Q), FP64. */
 int lbm_get_distributions(lbm_handle* h, double* f);
 
@@ -237,6 +282,43 @@ int lbm_get_particles(lbm_handle* h, lbm_particle_state* out, int32_t capacity, 
 /* Overwrite position / velocity / angular velocity / swimming direction of
  * particle `id` (1-based) and re-voxelise it (moveParticles! initialSetup). */
 int lbm_set_particle(lbm_handle* h, int32_t id, const lbm_particle_state* s);
+
+/* Report the momentum-exchange force (last_force) of particle `id` even when
+ * it is not coupled to forces, without applying it: the drag on a held
+ * particle.  No counterpart in the reference, which accumulates no force for
+ * an uncoupled particle (src/gpu/fluids.jl:198-202); off by default. */
+int lbm_record_force(lbm_handle* h, int32_t id, int32_t on);
+
+/* ---- particle-particle interactions (molecularDynamicsTick!,
+ * src/gpu/particles.jl:100-197; set-up src/gpu/initMethods.jl:224-414) ------
+ * Every tick, after the hydrodynamic update and before the particles move,
+ * each interaction adds its forces to the force input of its particles, from
+ * their positions before the move; the particle update then applies force
+ * input and momentum exchange together (coupled particles only).  The list
+ * replaces any previous one; pair interactions (Lennard-Jones, WCA, dipoles)
+ * come as one entry per pair, in the reference's order (the pairs (i, j),
+ * i < j, of each interaction, interactions in the order they were added).
+ * Parameters p[]:
+ *   LINEAR        bond: p0 equilibrium displacement, p1 stiffness
+ *   BISTABLE      p0 trap radius, p1 a, p2 b (force (a (d-R)^3 - b (d-R)) r^)
+ *   POLAR         three particles id1-id2-id3: p0 equilibrium angle, p1 stiffness
+ *   LENNARD_JONES p0 epsilon, p1 sigma, p2 cutoff (a WCA potential: cutoff 2^(1/6) sigma)
+ *   DIPOLE        p0 dipole constant, p1..p3 magnetic field (the front end evaluates
+ *                 a time-dependent field and sets the list again)
+ * Not with the CPU module's particle rules (the CPU module has no
+ * interactions), the persistent tick schedule (the tick runs in stream order
+ * instead), batches or lbm_adjoint. */
+#define LBM_INTERACTION_LINEAR 0
+#define LBM_INTERACTION_BISTABLE 1
+#define LBM_INTERACTION_POLAR 2
+#define LBM_INTERACTION_LENNARD_JONES 3
+#define LBM_INTERACTION_DIPOLE 4
+typedef struct lbm_interaction {
+    int32_t kind;
+    int32_t id1, id2, id3;  /* 1-based particle ids (id3: POLAR only) */
+    double p[4];
+} lbm_interaction;
+int lbm_set_interactions(lbm_handle* h, const lbm_interaction* list, int32_t n);
 
 /* particle.boundaryConditionsParams.solidRegion (N...) as 0/1 bytes
  * (getSphere, src/gpu/aux.jl:206-215), for particle `id` (1-based). */
@@ -370,8 +452,9 @@ void lbm_batch_destroy(lbm_batch* b);
 
 /* ---- gradients: discrete adjoint with binomial checkpointing --------------
  * Observable: the time average, over ticks window_begin..window_end (after
- * that many ticks, 1-based, inclusive), of the particle's velocity along
- * `direction` (zero vector: its initial swimming direction), over a run of
+ * that many ticks, 1-based, inclusive), of the particle's velocity or of the
+ * momentum-exchange force on it (spec.observable) along `direction` (zero
+ * vector: its initial swimming direction), over a run of
  * `ticks` ticks from the handle's initial state (tick 0).  Returns its value
  * and its derivatives with respect to the particle's B1 and B2, the
  * relaxation time tau (tau+ with tau- following: dtau = dtau_plus +
@@ -390,8 +473,19 @@ typedef struct lbm_adjoint_spec {
     double direction[3];
     double tau_minus_slope;
     int32_t snapshots;    /* stored states, including the initial one (>= 2) */
-    int32_t reserved;
+    int32_t observable;   /* LBM_OBSERVABLE_* */
 } lbm_adjoint_spec;
+
+/* Observables of lbm_adjoint, each averaged over the window along `direction`:
+ *   VELOCITY  the particle's velocity (its swimming speed)
+ *   FORCE     the momentum-exchange force of the tick (src/gpu/fluids.jl:191-205);
+ *             for a held particle (coupleForces false, which the reference does
+ *             not move) this is its drag: the force is accumulated for the
+ *             observable only, never applied, and ordinary lbm_step calls keep
+ *             reporting zero force for such a particle, as the reference does */
+/* (lbm_record_force makes the same force visible in ordinary stepping) */
+#define LBM_OBSERVABLE_VELOCITY 0
+#define LBM_OBSERVABLE_FORCE 1
 
 typedef struct lbm_adjoint_result {
     double value;         /* the observable */

@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(const AdjArgs a) {
                 const double s = 2.0 * fs[i] + w6 * rho * cu;  // f*_i + f^{n+1}_j
                 const double lj = a.lam_in[j * N + cell];
                 double lsi = lj, gmu = lj * w6 * cu, gup = lj * w6 * rho;  // lam_up = gup * c_j
-                if (P.coupleF) {
+                if (P.coupleF || P.recordF) {
                     const double t = a.coeff * (a.lamF[0] * ci[0] + a.lamF[1] * ci[1] + a.lamF[2] * ci[2]);
                     lsi += 2.0 * t;
                     gmu += t * w6 * cu;

@@ -15,6 +15,10 @@ struct CodecArgs {
     double rho0, scale, inv_scale, half_dt;
     double F[3];
     int force_mode;
+    double* stress;       // [d][d][N] viscous stress tensor (k_stress) or null
+    double stress_coeff;  // 1 - dt/(2 tau)
+    int incompressible;
+    double rho_inc;       // rho0 of the incompressible equilibrium
 };
 
 // f (FP64, reference units) -> stored g = (f/w - rho0)*scale
@@ -86,6 +90,61 @@ __global__ void k_macro(const CodecArgs a) {
         for (int k = 0; k < L::D; ++k) a.u[k * a.N + c] = rho == 0.0 ? 0.0 : (j[k] + a.half_dt * F[k]) / rho;
 }
 
+
+// viscousStressTensor (src/cpu/fluids.jl:507-520; commented out in the GPU
+// module, src/gpu/fluids.jl:272-285) from the stored populations, in FP64:
+//   sigma_ab = -(1 - dt/(2 tau)) sum_i c_ia c_ib (f_i - f_eq_i(rho, u))
+// with rho and u of hydroVariablesUpdate! (u with the Guo half force) and the
+// equilibrium of equilibriumDistribution (src/gpu/fluids.jl:39-52).  Wall
+// nodes hold f = 0, rho = u = 0, hence sigma = 0.
+template <class L, int ST>
+__global__ void k_stress(const CodecArgs a) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    constexpr int D = L::D;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    const T* pop = static_cast<const T*>(a.pop);
+    const bool wall = a.wall && a.wall[c];
+    double f[L::Q];
+    double rho = 0.0, j[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        f[i] = wall ? 0.0 : L::w(i) * (a.rho0 + (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale));
+        rho += f[i];
+        j[0] += L::cx(i) * f[i];
+        j[1] += L::cy(i) * f[i];
+        j[2] += L::cz(i) * f[i];
+    }
+    double F[3] = {0, 0, 0};
+    if (!wall) {
+        if (a.force_mode == 1) {
+            F[0] = a.F[0];
+            F[1] = a.F[1];
+            F[2] = a.F[2];
+        } else if (a.force_mode == 2) {
+            for (int k = 0; k < D; ++k) F[k] = a.ffield[k * a.N + c];
+        }
+    }
+    double u[3] = {0, 0, 0};
+    if (rho != 0.0)
+        for (int k = 0; k < D; ++k) u[k] = (j[k] + a.half_dt * F[k]) / rho;
+    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    double s[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const double uc = u[0] * L::cx(i) + u[1] * L::cy(i) + u[2] * L::cz(i);
+        const double second = uc * 3.0 + uc * uc * 4.5 - uu * 1.5;
+        const double feq = a.incompressible ? L::w(i) * rho + L::w(i) * (a.rho_inc * second)
+                                            : L::w(i) * ((second + 1.0) * rho);
+        const double fneq = f[i] - feq;
+        const int ci[3] = {L::cx(i), L::cy(i), L::cz(i)};
+        for (int p = 0; p < D; ++p)
+            for (int q = 0; q < D; ++q) s[p][q] += ci[p] * ci[q] * fneq;
+    }
+    for (int p = 0; p < D; ++p)
+        for (int q = 0; q < D; ++q) a.stress[(p + D * q) * a.N + c] = -a.stress_coeff * s[p][q];
+}
 
 struct InitArgs {
     void* pop;

@@ -120,7 +120,7 @@ inline int tma_smem_bytes(int q, int nx, int rows, int stages, int esz) {
     return (int)(((data + 15) / 16) * 16 + 8 * kTmaMaxStages);
 }
 
-template <class L, int ST, bool TRT>
+template <class L, int ST, bool TRT, bool SR>
 __global__ void __launch_bounds__(512, 1) k_bulk_tma(const StepArgs a, const int rows_max, const int stages) {
     extern __shared__ __align__(128) unsigned char smem[];
     using T = typename Store<ST>::T;
@@ -196,6 +196,11 @@ __global__ void __launch_bounds__(512, 1) k_bulk_tma(const StepArgs a, const int
 #pragma unroll
         for (int c = 0; c < 4; ++c) bad |= bad_density(collide<L, R, TRT>(a, g[c], Fx, Fy, Fz, false));
         report_density(valid && bad, a.err);
+        constexpr bool sr = SR && Store<ST>::bytes == 2;
+        unsigned dw[4];
+        if (sr) dither_words<Store<ST>::drop>(group_dither((int)(x0 + nx * (y + (long long)ny * z)), g[0][1], g[0][2],
+                                                           g[0][3]), dw);
+        const unsigned* dither = sr ? dw : nullptr;
         const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
         const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
         const int left = (j + RT - 1) & (RT - 1), right = (j + 1) & (RT - 1);
@@ -203,13 +208,13 @@ __global__ void __launch_bounds__(512, 1) k_bulk_tma(const StepArgs a, const int
         for (int i = 0; i < Q; ++i) {
             const int tq = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
             if (L::cx(i) == 0) {
-                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, g[0][i], g[1][i], g[2][i], g[3][i]);
+                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, g[0][i], g[1][i], g[2][i], g[3][i], dither);
             } else if (L::cx(i) == 1) {
                 const R in = __shfl_sync(lanes, g[3][i], left, RT);
-                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, in, g[0][i], g[1][i], g[2][i]);
+                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, in, g[0][i], g[1][i], g[2][i], dither);
             } else {
                 const R in = __shfl_sync(lanes, g[0][i], right, RT);
-                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, g[1][i], g[2][i], g[3][i], in);
+                if (valid) Vec4<ST>::store(a.dstq[i], tq, i, g[1][i], g[2][i], g[3][i], in, dither);
             }
         }
     }

@@ -33,12 +33,16 @@ __device__ __forceinline__ void ladd_link(const StepArgs& a, const ParticleDev& 
                                           int ci2, const double* Tc, const double* Xc, double rhoL, double gi,
                                           double wi, double& v, double* acc) {
     double up[3];
-    slip_velocity<D>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, Tc[0], Tc[1], Tc[2], up);
+    if (P.rules == 1)  // LBM_RULES_CPU_MODULE: uw = u_p(x) + u_p(x - c), u_p(x) = 0 at the fluid node x
+        slip_velocity_cpu<D>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, P.radius, 2.0 * a.half_dt, Tc[0], Tc[1],
+                             Tc[2], up);
+    else
+        slip_velocity<D>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, Tc[0], Tc[1], Tc[2], up);
     v += 6.0 * rhoL * (-(ci0 * up[0] + ci1 * up[1] + ci2 * up[2]));
-    if (owner && (P.coupleF || P.coupleT)) {
+    if (owner && (P.coupleF || P.coupleT || P.recordF)) {
         // f*_i(x) + f_j(x) in f units; F -= coeff*s*c_j = coeff*s*c_i
         const double cs = a.coeff * (wi * (2.0 * a.rho0 + gi + v));
-        if (P.coupleF) {
+        if (P.coupleF || P.recordF) {
             acc[0] += cs * ci0;
             acc[1] += cs * ci1;
             acc[2] += cs * ci2;
@@ -280,7 +284,8 @@ __device__ __forceinline__ bool fixup_body(const StepArgs& a, const long long b)
     for (int l = tid; l < nlist; l += NT) {
         const int item = s_list[l];
         dst[(item & 31) * N + s_cell[item >> 5]] =
-            SS::enc_sr(s_val[l], R(a.scale), (unsigned)s_cell[item >> 5], item & 31);
+            a.stochastic ? SS::enc_sr(s_val[l], R(a.scale), (unsigned)s_cell[item >> 5], item & 31)
+                         : SS::enc(s_val[l], R(a.scale));
     }
     if (!is_part) return true;
     // fixed-order reduction: butterfly inside warps, warps summed in order

@@ -85,7 +85,11 @@ struct ParticleDev {
     int nlinks;              // entries in use
     int part_off;            // partial-sum slots: one per chunk of kFixBlock entries
     int relink;              // the link list must be rebuilt (k_links, k_links_sort) before the next fix-up
-    int pad1;
+    int rules;               // LBM_RULES_* of the model: which module's particle update and node velocity
+    int recordF;             // accumulate the momentum-exchange force even when coupleF is off (the
+                             // adjoint's force observable; the force is reported, never applied)
+    int pad2;
+    long long nrec;          // ticks recorded into the trajectory ring (ParticleArgs::trj)
 };
 
 // Collision constants in one precision (see collide()), derived on the host
@@ -147,6 +151,7 @@ struct StepArgs {
     double gA[27], gB[27];
     double gK0, gkA, gkB;
     int trt;                              // collision model of the constants below (0 BGK, 1 TRT)
+    int stochastic;                       // 2-byte storage: 1 stochastic rounding of the stores, 0 nearest
     CollideK<float> kf;                   // the constants in FP32 and FP64 (fill_collide_consts)
     CollideK<double> kd;
     // per-direction population planes of src / dst (vector bulk kernel)
@@ -286,6 +291,51 @@ __device__ __forceinline__ void slip_velocity(const double* sR, const double* sV
     double edr = ur[0] * sE[0] + ur[1] * sE[1] + (D == 3 ? ur[2] * sE[2] : 0.0);
     double first = B1 + B2 * edr;
     for (int k = 0; k < 3; ++k) out[k] = first * (edr * ur[k] - (k < D ? sE[k] : 0.0)) + bulk[k];
+}
+
+// bulkVelocity of the reference's CPU module at one solid node
+// (src/cpu/particles.jl:21-46): v + cross(w, x - R) with the CPU module's cross
+// (src/cpu/aux.jl:19-28; in 2D the scalar w acts as (0, 0, w)), plus the slip
+// (B1 + B2 e.r)((e.r) r - e) with r = (x - R)/|x - R|, the unit vector by a
+// division.  Nodes farther than 2 dx from the surface get zero (:25); a solid
+// node next to a fluid node lies within sqrt(d) dx of it, so no link does.
+template <int D>
+__device__ __forceinline__ void slip_velocity_cpu(const double* sR, const double* sV, const double* sW,
+                                                  const double* sE, double B1, double B2, int kind, double radius,
+                                                  double dx, double X0, double X1, double X2, double* out) {
+    const double xr[3] = {X0 - sR[0], X1 - sR[1], D == 3 ? X2 - sR[2] : 0.0};
+    const double mx = fmax(fabs(xr[0]), fmax(fabs(xr[1]), fabs(xr[2])));
+    double nrm = 0.0;
+    if (mx != 0.0) {
+        double s2 = xr[0] * xr[0];
+        s2 += xr[1] * xr[1];
+        if (D == 3) s2 += xr[2] * xr[2];
+        nrm = sqrt(s2);
+    }
+    out[0] = out[1] = out[2] = 0.0;
+    if (fabs(nrm - radius) > 2.0 * dx) return;
+    double bulk[3];
+    if (D == 2) {
+        bulk[0] = sV[0] + (0.0 - sW[0] * xr[1]);
+        bulk[1] = sV[1] + (sW[0] * xr[0]);
+        bulk[2] = 0.0;
+    } else {
+        bulk[0] = sV[0] + (sW[1] * xr[2] - sW[2] * xr[1]);
+        bulk[1] = sV[1] + (-sW[0] * xr[2] + sW[2] * xr[0]);
+        bulk[2] = sV[2] + (sW[0] * xr[1] - sW[1] * xr[0]);
+    }
+    if (kind == 0 || nrm == 0.0) {
+        out[0] = bulk[0];
+        out[1] = bulk[1];
+        out[2] = bulk[2];
+        return;
+    }
+    double fr[3] = {xr[0] / nrm, xr[1] / nrm, D == 3 ? xr[2] / nrm : 0.0};
+    double edr = sE[0] * fr[0];
+    edr += sE[1] * fr[1];
+    if (D == 3) edr += sE[2] * fr[2];
+    const double first = B1 + B2 * edr;
+    for (int k = 0; k < D; ++k) out[k] = first * (edr * fr[k] - sE[k]) + bulk[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -455,7 +505,7 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int t = xs[L::cx(i) + 1] + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
-        dst[i * N + t] = SS::enc_sr(s.g[i], R(1), (unsigned)t, i);
+        dst[i * N + t] = a.stochastic ? SS::enc_sr(s.g[i], R(1), (unsigned)t, i) : SS::enc(s.g[i], R(1));
     }
 }
 
@@ -474,7 +524,8 @@ template <> struct Vec4<ST_F32> {
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     }
     // values of direction `dir` for cells cell0 .. cell0+3 (cell0 a multiple of 4)
-    static __device__ __forceinline__ void store(void* base, int cell0, int, float a0, float a1, float a2, float a3) {
+    static __device__ __forceinline__ void store(void* base, int cell0, int, float a0, float a1, float a2, float a3,
+                                                 const unsigned*) {
         // streaming (evict-first) store: the next read of the line is a tick away,
         // after the pass has streamed far more than L2 through the cache
         __stcs(reinterpret_cast<float4*>(static_cast<float*>(base) + cell0), make_float4(a0, a1, a2, a3));
@@ -487,16 +538,20 @@ template <> struct Vec4<ST_F16> {
         const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
+    // rounding to nearest (dither null) or stochastic with the group's dither
+    // words (storage.cuh): cell k of direction dir adds word (k + dir) mod 4
     static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
-                                                 float a3) {
-        const unsigned key = (unsigned)cell0 * kDitherCell;  // stochastic rounding (storage.cuh)
-        const __half2 lo = __floats2half2_rn(round_dither<13>(a0, key, dither_mul(dir, 0)),
-                                             round_dither<13>(a1, key, dither_mul(dir, 1)));
-        const __half2 hi = __floats2half2_rn(round_dither<13>(a2, key, dither_mul(dir, 2)),
-                                             round_dither<13>(a3, key, dither_mul(dir, 3)));
+                                                 float a3, const unsigned* dither) {
         uint2 q;
-        q.x = *reinterpret_cast<const unsigned*>(&lo);
-        q.y = *reinterpret_cast<const unsigned*>(&hi);
+        if (dither) {
+            q.x = pack_half2_rz(add_dither(a0, dither[dir & 3]), add_dither(a1, dither[(dir + 1) & 3]));
+            q.y = pack_half2_rz(add_dither(a2, dither[(dir + 2) & 3]), add_dither(a3, dither[(dir + 3) & 3]));
+        } else {
+            const __half2 lo = __floats2half2_rn(a0, a1);
+            const __half2 hi = __floats2half2_rn(a2, a3);
+            q.x = *reinterpret_cast<const unsigned*>(&lo);
+            q.y = *reinterpret_cast<const unsigned*>(&hi);
+        }
         __stcs(reinterpret_cast<uint2*>(static_cast<__half*>(base) + cell0), q);  // streaming, as above
     }
 };
@@ -508,15 +563,17 @@ template <> struct Vec4<ST_BF16> {
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
     }
     static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
-                                                 float a3) {
-        const unsigned key = (unsigned)cell0 * kDitherCell;  // stochastic rounding (storage.cuh)
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(round_dither<16>(a0, key, dither_mul(dir, 0)),
-                                                        round_dither<16>(a1, key, dither_mul(dir, 1)));
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(round_dither<16>(a2, key, dither_mul(dir, 2)),
-                                                        round_dither<16>(a3, key, dither_mul(dir, 3)));
+                                                 float a3, const unsigned* dither) {
         uint2 q;
-        q.x = *reinterpret_cast<const unsigned*>(&lo);
-        q.y = *reinterpret_cast<const unsigned*>(&hi);
+        if (dither) {
+            q.x = pack_bf162_rz(add_dither(a0, dither[dir & 3]), add_dither(a1, dither[(dir + 1) & 3]));
+            q.y = pack_bf162_rz(add_dither(a2, dither[(dir + 2) & 3]), add_dither(a3, dither[(dir + 3) & 3]));
+        } else {
+            const __nv_bfloat162 lo = __floats2bfloat162_rn(a0, a1);
+            const __nv_bfloat162 hi = __floats2bfloat162_rn(a2, a3);
+            q.x = *reinterpret_cast<const unsigned*>(&lo);
+            q.y = *reinterpret_cast<const unsigned*>(&hi);
+        }
         __stcs(reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(base) + cell0), q);  // streaming, as above
     }
 };
@@ -534,6 +591,7 @@ constexpr int x_slot(int i) {  // exchange slot of direction i (cx != 0)
     return n;
 }
 
+
 // One tile of the vector bulk pass: `a.vrows` full x-rows of one z-slice, four
 // consecutive x-nodes per thread with 128-bit (FP32) or 64-bit (FP16/BF16)
 // loads and stores.  Because a CTA owns whole x-rows, the periodic x-wrap
@@ -541,7 +599,9 @@ constexpr int x_slot(int i) {  // exchange slot of direction i (cx != 0)
 // value per row segment that crosses into the neighbouring thread goes
 // through shared memory, and every global store is an aligned vector store.
 // Threads past the tile's rows only take part in the barrier.
-template <class L, int ST, bool TRT, int B>
+// SR: the 2-byte stores round stochastically (a separate instantiation, so
+// that the nearest-rounding kernels keep their register allocation)
+template <class L, int ST, bool TRT, int B, bool SR = false>
 __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, float (*s_ex)[B]) {
     using R = float;
     constexpr int Q = L::Q;
@@ -571,6 +631,10 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
 #pragma unroll
     for (int k = 0; k < 4; ++k) bad |= bad_density(collide<L, R, TRT>(a, g[k], Fx, Fy, Fz, false));
     report_density(valid && bad, a.err);
+    constexpr bool sr = SR && Store<ST>::bytes == 2;
+    unsigned dw[4];
+    if (sr) dither_words<Store<ST>::drop>(group_dither(cell0, g[0][1], g[0][2], g[0][3]), dw);
+    const unsigned* dither = sr ? dw : nullptr;
     // the value of each +-x direction that leaves this thread's 4-node segment
     if (row < a.vrows) {
 #pragma unroll
@@ -589,11 +653,11 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
     for (int i = 0; i < Q; ++i) {
         const int t0 = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
         if (L::cx(i) == 0) {
-            Vec4<ST>::store(a.dstq[i], t0, i, g[0][i], g[1][i], g[2][i], g[3][i]);
+            Vec4<ST>::store(a.dstq[i], t0, i, g[0][i], g[1][i], g[2][i], g[3][i], dither);
         } else if (L::cx(i) == 1) {
-            Vec4<ST>::store(a.dstq[i], t0, i, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i]);
+            Vec4<ST>::store(a.dstq[i], t0, i, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i], dither);
         } else {
-            Vec4<ST>::store(a.dstq[i], t0, i, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right]);
+            Vec4<ST>::store(a.dstq[i], t0, i, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right], dither);
         }
     }
 }
@@ -604,15 +668,19 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
 // memory-bound, and up to 96 (20 warps per SM) with 2-byte storage, whose
 // conversions make it issue-bound as well: the extra warps took its 128^3
 // pass from 28.4 to 26.9 us, with no change for FP32.
-template <class L, int ST = ST_F32>
-constexpr int bulk_threads_per_sm() { return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? 640 : 512); }
+// With stochastic rounding the 2-byte kernels keep the dither word and its
+// arithmetic in registers: 18 warps per SM (112 registers) instead of 20.
+template <class L, int ST = ST_F32, bool SR = false>
+constexpr int bulk_threads_per_sm() {
+    return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? (SR ? 576 : 640) : 512);
+}
 
 // the vector bulk pass over all tiles, one CTA of B threads per tile
-template <class L, int ST, bool TRT, int B>
-__global__ void __launch_bounds__(B, bulk_threads_per_sm<L, ST>() / B) k_bulk_v4(const StepArgs a) {
+template <class L, int ST, bool TRT, int B, bool SR>
+__global__ void __launch_bounds__(B, bulk_threads_per_sm<L, ST, SR>() / B) k_bulk_v4(const StepArgs a) {
     __shared__ float s_ex[x_moving_dirs<L>()][B];
     grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
-    bulk_v4_tile<L, ST, TRT, B>(a, blockIdx.x, s_ex);
+    bulk_v4_tile<L, ST, TRT, B, SR>(a, blockIdx.x, s_ex);
 }
 
 // periodic intervals [a0, a0+la) and [b0, b0+lb) of an axis of n nodes meet

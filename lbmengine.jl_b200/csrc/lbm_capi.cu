@@ -8,13 +8,17 @@
 // k_particles on a side stream (see enqueue_tick).
 #include "lbm_b200.h"
 #include "ops.cuh"
+#include "interactions.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <charconv>
 #include <chrono>
+#include <thread>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -54,6 +58,8 @@ struct lbm_handle {
     double dx = 1, dt = 1, tau = 1, tau_minus = 1;
     double rho0 = 1, scale = 1;
     int force_mode = 0;
+    int particle_rules = LBM_RULES_GPU_MODULE;
+    int rounding = LBM_ROUND_STOCHASTIC;
     double F[3] = {0, 0, 0};
     int incompressible = 0;
     double rho_inc = 1;
@@ -68,6 +74,7 @@ struct lbm_handle {
     int vrows = 0, vnt1 = 0, vblock = 0;
     // TMA bulk pass (bulk_tma.cuh): its launch shape, valid when tma_ok
     int bulk_kind = LBM_BULK_AUTO;
+    bool in_batch = false;  // a replica of an lbm_batch: its tiles belong to the batch's queue
     TmaShape tma{};
     bool tma_ok = false;
     long long vtiles = 0;
@@ -111,6 +118,19 @@ struct lbm_handle {
     long long linkcnt_slots = 0;
     int* d_err = nullptr;
     double* d_tmp = nullptr;  // FP64 read-back / upload scratch
+    // particle interactions (lbm_set_interactions)
+    std::vector<lbm_interaction> inter;
+    InterItem* d_items = nullptr;
+    int* d_coff = nullptr;
+    int* d_cent = nullptr;
+    double* d_pf = nullptr;
+    double* d_fint = nullptr;
+    // trajectory recording (lbm_record_trajectories): ring of trj_cap ticks
+    double* d_trj = nullptr;
+    long long trj_cap = 0, trj_read = 0;
+    // asynchronous writer of fluid snapshots (lbm_write_fluid_csv)
+    std::thread writer;
+    std::string writer_err;
     size_t tmp_bytes = 0;
     size_t device_bytes = 0;
     // time
@@ -346,6 +366,7 @@ StepArgs make_step_args(const lbm_handle* h, int src, double* partial) {
         a.dstq[i] = static_cast<char*>(a.dst) + (size_t)i * h->N * esz;
     }
     a.trt = h->trt;
+    a.stochastic = h->rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
     fill_collide_consts(a);
     return a;
 }
@@ -366,7 +387,8 @@ bool use_tma_bulk(const lbm_handle* h) {
 // rows of nx = 4 RT nodes with RT a power of two up to 32 (a row is a
 // shuffle segment of a warp), 16-byte aligned rows, no per-node force field.
 bool choose_tma(lbm_handle* h, int threads, int stages, TmaShape* out) {
-    if (!h->ops.bulk_tma || !h->ops.bulk_tma_fn || h->force_mode == LBM_FORCE_FIELD) return false;
+    const void* fn = h->rounding == LBM_ROUND_STOCHASTIC ? h->ops.bulk_tma_fn_sr : h->ops.bulk_tma_fn;
+    if (!h->ops.bulk_tma || !fn || h->force_mode == LBM_FORCE_FIELD) return false;
     const int nx = h->n[0], ny = h->n[1], esz = storage_bytes(h->storage);
     if (nx % 4 != 0) return false;
     const int RT = nx / 4;
@@ -383,12 +405,12 @@ bool choose_tma(lbm_handle* h, int threads, int stages, TmaShape* out) {
     if (stages < 2 || stages > kTmaMaxStages) return false;
     const int smem = tma_smem_bytes(h->q, nx, rows, stages, esz);
     if (smem > 227 * 1024) return false;
-    if (cudaFuncSetAttribute(h->ops.bulk_tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h->ops.bulk_tma_fn, threads, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         return false;
@@ -435,7 +457,30 @@ ParticleArgs particle_args(const lbm_handle* h, int mode, int pid, int src = -1)
     a.dx = h->dx;
     a.dt = h->dt;
     a.err = h->d_err;
+    a.trj = h->d_trj;
+    a.trj_cap = h->trj_cap;
+    a.fint = h->inter.empty() ? nullptr : h->d_fint;
     return a;
+}
+
+InterArgs inter_args(const lbm_handle* h) {
+    InterArgs a{};
+    a.items = h->d_items;
+    a.nitems = (int)h->inter.size();
+    a.nparts = (int)h->hparts.size();
+    a.dims = h->dims;
+    a.parts = h->d_parts;
+    a.coff = h->d_coff;
+    a.cent = h->d_cent;
+    a.pf = h->d_pf;
+    a.fint = h->d_fint;
+    return a;
+}
+
+// the interactions of a tick, before its particle update (same stream)
+void launch_interactions(const lbm_handle* h, cudaStream_t s) {
+    if (h->inter.empty()) return;
+    k_interactions<<<1, kInterThreads, 0, s>>>(inter_args(h));
 }
 
 CodecArgs codec_args(const lbm_handle* h) {
@@ -472,7 +517,7 @@ long long fixup_grid(const lbm_handle* h) {
 // the persistent tick kernel applies to the vector bulk kernel with
 // kTickBlock-thread tiles, when there is boundary work to overlap
 bool use_tick_kernel(const lbm_handle* h) {
-    return h->schedule == LBM_SCHEDULE_PERSISTENT && use_vector_bulk(h) && h->ops.tick != nullptr &&
+    return h->schedule == LBM_SCHEDULE_PERSISTENT && h->inter.empty() && use_vector_bulk(h) && h->ops.tick != nullptr &&
            h->vblock == kTickBlock && h->tick_grid > 0 && fixup_blocks(h) > 0;
 }
 
@@ -599,7 +644,8 @@ void programmatic_from(cudaStream_t s, cudaGraphNode_t from) {
 void enqueue_tick(lbm_handle* h, int src, int slot) {
     prof_record(h, slot, 0, h->stream);
     if (use_tick_kernel(h)) {
-        h->ops.tick(h->d_targs + src, h->d_pargs + src, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
+        h->ops.tick(h->d_targs + src, h->d_pargs + src, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream,
+                    h->rounding == LBM_ROUND_STOCHASTIC);
         prof_record(h, slot, 1, h->stream);
         return;
     }
@@ -631,6 +677,7 @@ void enqueue_tick(lbm_handle* h, int src, int slot) {
         prof_record(h, slot, 2, h->side);
         ParticleArgs pa = particle_args(h, 0, 0, src);
         pa.inline_links = 1;
+        launch_interactions(h, h->side);
         h->ops.particles(pa, (unsigned)a.nparts, h->side);
         prof_record(h, slot, 3, h->side);
         cudaEventRecord(h->ev_part, h->side);
@@ -747,7 +794,14 @@ int upload(lbm_handle* h, void* dst, const void* src, size_t bytes) {
 
 void destroy_all(lbm_handle* h) {
     if (!h) return;
+    if (h->writer.joinable()) h->writer.join();
     cudaSetDevice(h->device);
+    dev_free(h->d_trj);
+    dev_free(h->d_items);
+    dev_free(h->d_coff);
+    dev_free(h->d_cent);
+    dev_free(h->d_pf);
+    dev_free(h->d_fint);
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     dev_free(h->pop[0]);
@@ -860,6 +914,132 @@ bool is_uniform_axis(const std::vector<double>& X, double dx) {
     return true;
 }
 
+// (Re)allocate the trajectory ring for `cap` ticks of every particle and
+// restart the count; cap 0 stops recording.
+int trj_alloc(lbm_handle* h, long long cap) {
+    if (h->d_trj) {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        dev_free(h->d_trj);
+        h->device_bytes -= sizeof(double) * 9 * (size_t)h->trj_cap * h->hparts.size();
+    }
+    h->trj_cap = 0;
+    h->trj_read = 0;
+    const long long np = (long long)h->hparts.size();
+    for (long long p = 0; p < np; ++p) {
+        const long long zero = 0;
+        CUDA_TRY(h, cudaMemcpyAsync(&h->d_parts[p].nrec, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    }
+    if (cap > 0 && np > 0) {
+        const int rc = dev_alloc(h, &h->d_trj, sizeof(double) * 9 * (size_t)cap * np);
+        if (rc) return rc;
+        h->trj_cap = cap;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);  // the graphs hold the particle kernel's arguments
+    return LBM_OK;
+}
+
+// Upload the interaction items and each particle's ordered contributions.
+int upload_interactions(lbm_handle* h) {
+    const int n = (int)h->inter.size(), np = (int)h->hparts.size();
+    dev_free(h->d_items);
+    dev_free(h->d_coff);
+    dev_free(h->d_cent);
+    dev_free(h->d_pf);
+    dev_free(h->d_fint);
+    if (n == 0) return LBM_OK;
+    std::vector<InterItem> items(n);
+    std::vector<std::vector<int>> per(np);
+    for (int t = 0; t < n; ++t) {
+        const lbm_interaction& e = h->inter[t];
+        InterItem& it = items[t];
+        it.kind = e.kind;
+        it.id1 = e.id1 - 1;
+        it.id2 = e.id2 - 1;
+        it.id3 = e.kind == LBM_INTERACTION_POLAR ? e.id3 - 1 : 0;
+        for (int k = 0; k < 4; ++k) it.p[k] = e.p[k];
+        // the order in which applyInteraction! adds to the force inputs
+        if (e.kind == LBM_INTERACTION_POLAR) {
+            per[it.id1].push_back(t << 3 | 0 << 1 | 0);
+            per[it.id3].push_back(t << 3 | 1 << 1 | 0);
+            per[it.id2].push_back(t << 3 | 2 << 1 | 1);
+        } else {
+            per[it.id1].push_back(t << 3 | 0 << 1 | 0);
+            per[it.id2].push_back(t << 3 | 0 << 1 | 1);
+        }
+    }
+    std::vector<int> coff(np + 1, 0), cent;
+    for (int p = 0; p < np; ++p) {
+        coff[p + 1] = coff[p] + (int)per[p].size();
+        cent.insert(cent.end(), per[p].begin(), per[p].end());
+    }
+    int rc = dev_alloc(h, &h->d_items, sizeof(InterItem) * n);
+    if (!rc) rc = dev_alloc(h, &h->d_coff, sizeof(int) * (np + 1));
+    if (!rc) rc = dev_alloc(h, &h->d_cent, sizeof(int) * std::max<size_t>(1, cent.size()));
+    if (!rc) rc = dev_alloc(h, &h->d_pf, sizeof(double) * 9 * n);
+    if (!rc) rc = dev_alloc(h, &h->d_fint, sizeof(double) * 3 * std::max(1, np));
+    if (rc) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_items, items.data(), sizeof(InterItem) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_coff, coff.data(), sizeof(int) * (np + 1), cudaMemcpyHostToDevice, h->stream));
+    if (!cent.empty())
+        CUDA_TRY(h, cudaMemcpyAsync(h->d_cent, cent.data(), sizeof(int) * cent.size(), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+// Julia's print(::Float64) (what CSV.jl writes): the shortest digits that
+// read back to x; plain notation for 1e-4 <= |x| < 1e6 with at least one
+// decimal ("1.0", "0.0001"), else d.ddd e<exp> without padding ("1.0e-5",
+// "1.234567e6"); "NaN", "Inf", "-Inf".
+void julia_float(double x, std::string& out) {
+    if (std::isnan(x)) {
+        out += "NaN";
+        return;
+    }
+    if (std::isinf(x)) {
+        out += x < 0 ? "-Inf" : "Inf";
+        return;
+    }
+    if (x == 0.0) {
+        out += std::signbit(x) ? "-0.0" : "0.0";
+        return;
+    }
+    char buf[48];
+    const auto r = std::to_chars(buf, buf + sizeof(buf), x, std::chars_format::scientific);
+    const std::string sci(buf, r.ptr);  // [-]d[.ddd]e[+-]XX
+    const size_t epos = sci.find('e');
+    const int e10 = std::atoi(sci.c_str() + epos + 1);
+    std::string mant = sci.substr(0, epos);
+    const bool neg = mant[0] == '-';
+    if (neg) mant.erase(0, 1);
+    std::string digits;
+    for (char c : mant)
+        if (c != '.') digits += c;
+    if (neg) out += '-';
+    if (e10 < -4 || e10 >= 6) {
+        out += digits[0];
+        out += '.';
+        out += digits.size() > 1 ? digits.substr(1) : std::string("0");
+        out += 'e';
+        out += std::to_string(e10);
+    } else if (e10 < 0) {
+        out += "0.";
+        out.append((size_t)(-e10 - 1), '0');
+        out += digits;
+    } else {
+        const size_t ip = (size_t)e10 + 1;  // digits before the point
+        if (digits.size() <= ip) {
+            out += digits;
+            out.append(ip - digits.size(), '0');
+            out += ".0";
+        } else {
+            out += digits.substr(0, ip);
+            out += '.';
+            out += digits.substr(ip);
+        }
+    }
+}
+
 // static wall lists: wall nodes, and fluid nodes with a wall source in some direction
 void wall_lists(const lbm_handle* h, const std::vector<unsigned char>& W, std::vector<int2>& wl,
                 std::vector<int>& wn) {
@@ -942,6 +1122,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         return set_err(nullptr, LBM_ERR_UNSUPPORTED, "incompressible equilibrium with a non-uniform initial density");
     if (cfg->particle_rules != LBM_RULES_GPU_MODULE && cfg->particle_rules != LBM_RULES_CPU_MODULE)
         return set_err(nullptr, LBM_ERR_INVALID, "unknown particle rules");
+    if (cfg->rounding != LBM_ROUND_STOCHASTIC && cfg->rounding != LBM_ROUND_NEAREST)
+        return set_err(nullptr, LBM_ERR_INVALID, "unknown rounding");
 
     lbm_handle* h = new lbm_handle();
     h->device = device;
@@ -961,6 +1143,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
                    ? (cfg->store_scale > 0 ? cfg->store_scale : 4096.0)
                    : 1.0;
     h->force_mode = cfg->force_mode;
+    h->particle_rules = cfg->particle_rules;
+    h->rounding = cfg->rounding;
     h->schedule = cfg->schedule == LBM_SCHEDULE_AUTO ? LBM_SCHEDULE_STREAM : cfg->schedule;
     if (cfg->force_mode == LBM_FORCE_UNIFORM)
         for (int k = 0; k < cfg->dims; ++k) h->F[k] = cfg->force[k];
@@ -1010,7 +1194,8 @@ int lbm_create(const lbm_config* cfg, lbm_handle** out) {
         TRY(set_err(h, LBM_ERR_CUDA, "memset failed"));
     if (h->vtiles > 0 && h->vblock == kTickBlock && h->ops.tick_fn) {  // persistent grid: all resident CTAs
         int per_sm = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h->ops.tick_fn, kTickBlock, 0) != cudaSuccess ||
+        const void* tfn = h->rounding == LBM_ROUND_STOCHASTIC ? h->ops.tick_fn_sr : h->ops.tick_fn;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tfn, kTickBlock, 0) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
             TRY(set_err(h, LBM_ERR_CUDA, "occupancy query failed"));
         h->tick_grid = (unsigned)std::max(0, per_sm * sms);
@@ -1183,6 +1368,7 @@ int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_ou
     P.coupleF = p->couple_forces ? 1 : 0;
     P.coupleT = p->couple_torques ? 1 : 0;
     P.valid = 0;
+    P.rules = h->particle_rules;
     for (int k = 0; k < 3; ++k) {
         P.slo[k] = 1;
         P.shi[k] = 0;
@@ -1226,6 +1412,14 @@ int lbm_add_particle(lbm_handle* h, const lbm_particle_params* p, int32_t* id_ou
     rc = grow(h, &h->d_linkcnt, &h->linkcnt_slots, (long long)(pid + 1) * h->link_bpp, 0);
     if (rc) return rc;
     drop_graphs(h);
+    if (!h->inter.empty()) {  // the contribution lists cover every particle
+        rc = upload_interactions(h);
+        if (rc) return rc;
+    }
+    if (h->trj_cap > 0) {  // the ring holds every particle: start it again with this one
+        rc = trj_alloc(h, h->trj_cap);
+        if (rc) return rc;
+    }
     // initial setup: moveParticles!(initialSetup = true)
     h->ops.particles(particle_args(h, 1, pid), 1, h->stream);
     CUDA_TRY(h, cudaGetLastError());
@@ -1339,9 +1533,21 @@ int lbm_set_bulk_kernel(lbm_handle* h, int32_t kind, int32_t threads, int32_t st
     if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
     if (kind != LBM_BULK_AUTO && kind != LBM_BULK_VECTOR && kind != LBM_BULK_TMA)
         return set_err(h, LBM_ERR_INVALID, "unknown bulk kernel");
+    if (h->in_batch) return set_err(h, LBM_ERR_STATE, "a batch replica's kernels belong to its batch");
     BIND(h);
     if (kind == LBM_BULK_VECTOR && !use_vector_bulk(h))
         return set_err(h, LBM_ERR_UNSUPPORTED, "the vector bulk kernel does not apply to this model");
+    if (kind == LBM_BULK_VECTOR && threads != 0) {  // CTA size of the vector kernel (tiles of whole x-rows)
+        const int RT = h->n[0] / 4;
+        if ((threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512) || threads < RT ||
+            threads % RT != 0 || h->schedule == LBM_SCHEDULE_PERSISTENT)
+            return set_err(h, LBM_ERR_UNSUPPORTED,
+                           "vector kernel CTAs hold whole x-rows: 32..512 threads, a multiple of nx/4 (stream schedule)");
+        h->vblock = threads;
+        h->vrows = std::max(1, std::min(threads / RT, h->n[1]));
+        h->vnt1 = (h->n[1] + h->vrows - 1) / h->vrows;
+        h->vtiles = (long long)h->vnt1 * h->n[2];
+    }
     if (kind != LBM_BULK_VECTOR) {
         TmaShape sh{};
         if (!choose_tma(h, threads, stages, &sh)) {
@@ -1408,7 +1614,8 @@ int lbm_time_kernel(lbm_handle* h, int32_t kernel, int32_t launches, double* avg
         } else if (kernel == LBM_KERNEL_FIXUP) {
             h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, false, fixup_walk(h));
         } else if (kernel == LBM_KERNEL_TICK) {
-            h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream);
+            h->ops.tick(h->d_targs + b, h->d_pargs + b, h->items, h->d_tq, h->d_err, h->tick_grid, h->stream,
+                        h->rounding == LBM_ROUND_STOCHASTIC);
             b = 1 - b;
         } else {
             const ParticleArgs pa = particle_args(h, 0, 0, b);
@@ -1450,6 +1657,142 @@ int lbm_get_fields(lbm_handle* h, double* rho, double* u) {
     if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, c.rho, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
     if (u) CUDA_TRY(h, cudaMemcpyAsync(u, c.u, sizeof(double) * h->N * h->dims, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_get_stress(lbm_handle* h, double* sigma) {
+    if (!h || !sigma) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    const size_t nb = sizeof(double) * h->N * h->dims * h->dims;
+    int rc = ensure_tmp(h, nb);
+    if (rc) return rc;
+    CodecArgs c = codec_args(h);
+    c.stress = h->d_tmp;
+    c.stress_coeff = 1.0 - 0.5 * h->dt / h->tau;
+    c.incompressible = h->incompressible;
+    c.rho_inc = h->rho_inc;
+    h->ops.stress(c, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(sigma, c.stress, nb, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_record_trajectories(lbm_handle* h, int64_t capacity) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (capacity < 0) return set_err(h, LBM_ERR_INVALID, "capacity must be non-negative");
+    BIND(h);
+    return trj_alloc(h, capacity);
+}
+
+int lbm_read_trajectories(lbm_handle* h, double* out, int64_t capacity, int64_t* ticks) {
+    if (!h || !ticks) return set_err(h, LBM_ERR_INVALID, "null argument");
+    BIND(h);
+    *ticks = 0;
+    if (h->trj_cap == 0 || h->hparts.empty()) return LBM_OK;
+    long long nrec = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&nrec, &h->d_parts[0].nrec, sizeof(nrec), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const long long n = nrec - h->trj_read;
+    *ticks = n;
+    if (!out) return LBM_OK;
+    if (n > h->trj_cap)
+        return set_err(h, LBM_ERR_STATE, "trajectory records were overwritten: " + std::to_string(n) +
+                                             " ticks since the last read, the ring holds " + std::to_string(h->trj_cap));
+    if (n > capacity) return set_err(h, LBM_ERR_INVALID, "output buffer holds fewer ticks than were recorded");
+    const size_t per = 9 * h->hparts.size();  // doubles per tick
+    for (long long t = h->trj_read; t < nrec;) {  // at most two contiguous pieces of the ring
+        const long long slot = t % h->trj_cap;
+        const long long len = std::min(nrec - t, h->trj_cap - slot);
+        CUDA_TRY(h, cudaMemcpyAsync(out + (t - h->trj_read) * per, h->d_trj + slot * per, sizeof(double) * per * len,
+                                    cudaMemcpyDeviceToHost, h->stream));
+        t += len;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->trj_read = nrec;
+    return LBM_OK;
+}
+
+int lbm_output_flush(lbm_handle* h) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (h->writer.joinable()) h->writer.join();
+    if (!h->writer_err.empty()) {
+        const std::string e = h->writer_err;
+        h->writer_err.clear();
+        return set_err(h, LBM_ERR_INVALID, e);
+    }
+    return LBM_OK;
+}
+
+// writeTrajectories (src/gpu/aux.jl:271-317): one row per node in column-major
+// order with tick, time, the 1-based node indices, coordinates, density,
+// velocity and the Q populations, as CSV.jl writes them.  The fields are read
+// back here; formatting and writing run on a host thread while the caller
+// goes on stepping.
+int lbm_write_fluid_csv(lbm_handle* h, const char* path) {
+    if (!h || !path) return set_err(h, LBM_ERR_INVALID, "null argument");
+    int rc = lbm_output_flush(h);  // one snapshot in flight at a time
+    if (rc) return rc;
+    BIND(h);
+    const long long N = h->N;
+    const int d = h->dims, q = h->q;
+    auto rho = std::make_shared<std::vector<double>>(N);
+    auto u = std::make_shared<std::vector<double>>((size_t)N * d);
+    auto f = std::make_shared<std::vector<double>>((size_t)N * q);
+    rc = lbm_get_fields(h, rho->data(), u->data());
+    if (!rc) rc = lbm_get_distributions(h, f->data());
+    if (rc) return rc;
+    std::vector<double> X[3] = {h->X[0], h->X[1], h->X[2]};
+    const int n[3] = {h->n[0], h->n[1], h->n[2]};
+    const long long tick = h->tick;
+    const double time = h->time;
+    const std::string file(path);
+    h->writer = std::thread([h, rho, u, f, X, n, N, d, q, tick, time, file]() {
+        FILE* fp = std::fopen(file.c_str(), "w");
+        if (!fp) {
+            h->writer_err = "cannot open " + file;
+            return;
+        }
+        static const char* ax = "xyz";
+        std::string line = "tick,time";
+        for (int a = 0; a < d; ++a) line += std::string(",id_") + ax[a];
+        for (int a = 0; a < d; ++a) line += std::string(",coordinate_") + ax[a];
+        line += ",massDensity";
+        for (int a = 0; a < d; ++a) line += std::string(",fluidVelocity_") + ax[a];
+        for (int i = 1; i <= q; ++i) line += ",f" + std::to_string(i);
+        line += '\n';
+        std::string head = std::to_string(tick) + ",";
+        julia_float(time, head);
+        bool ok = std::fputs(line.c_str(), fp) >= 0;
+        std::string buf;
+        buf.reserve(1 << 22);
+        for (long long c = 0; c < N && ok; ++c) {
+            const long long idx[3] = {c % n[0], (c / n[0]) % n[1], c / ((long long)n[0] * n[1])};
+            buf += head;
+            for (int a = 0; a < d; ++a) buf += "," + std::to_string(idx[a] + 1);
+            for (int a = 0; a < d; ++a) {
+                buf += ',';
+                julia_float(X[a][idx[a]], buf);
+            }
+            buf += ',';
+            julia_float((*rho)[c], buf);
+            for (int a = 0; a < d; ++a) {
+                buf += ',';
+                julia_float((*u)[(size_t)a * N + c], buf);
+            }
+            for (int i = 0; i < q; ++i) {
+                buf += ',';
+                julia_float((*f)[(size_t)i * N + c], buf);
+            }
+            buf += '\n';
+            if (buf.size() > (1 << 22) - 4096) {
+                ok = std::fwrite(buf.data(), 1, buf.size(), fp) == buf.size();
+                buf.clear();
+            }
+        }
+        if (ok && !buf.empty()) ok = std::fwrite(buf.data(), 1, buf.size(), fp) == buf.size();
+        if (std::fclose(fp) != 0 || !ok) h->writer_err = "short write to " + file;
+    });
     return LBM_OK;
 }
 
@@ -1534,6 +1877,43 @@ int lbm_set_particle(lbm_handle* h, int32_t id, const lbm_particle_state* s) {
     h->ops.particles(particle_args(h, 1, id - 1), 1, h->stream);
     CUDA_TRY(h, cudaGetLastError());
     return check_device_error(h);
+}
+
+int lbm_set_interactions(lbm_handle* h, const lbm_interaction* list, int32_t n) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    if (n < 0 || (n > 0 && !list)) return set_err(h, LBM_ERR_INVALID, "bad interaction list");
+    if (n > (1 << 26)) return set_err(h, LBM_ERR_UNSUPPORTED, "too many interaction items");
+    BIND(h);
+    if (n > 0 && h->particle_rules != LBM_RULES_GPU_MODULE)
+        return set_err(h, LBM_ERR_UNSUPPORTED, "the CPU module has no particle interactions");
+    const int np = (int)h->hparts.size();
+    for (int t = 0; t < n; ++t) {
+        const lbm_interaction& e = list[t];
+        if (e.kind < LBM_INTERACTION_LINEAR || e.kind > LBM_INTERACTION_DIPOLE)
+            return set_err(h, LBM_ERR_INVALID, "unknown interaction kind");
+        const bool three = e.kind == LBM_INTERACTION_POLAR;
+        if (e.id1 < 1 || e.id1 > np || e.id2 < 1 || e.id2 > np || (three && (e.id3 < 1 || e.id3 > np)) ||
+            e.id1 == e.id2 || (three && (e.id3 == e.id1 || e.id3 == e.id2)))
+            return set_err(h, LBM_ERR_INVALID, "interaction " + std::to_string(t + 1) + " names no valid particles");
+    }
+    h->inter.assign(list, list + n);
+    const int rc = upload_interactions(h);
+    if (rc) {
+        h->inter.clear();
+        return rc;
+    }
+    drop_graphs(h);  // the graphs hold the interaction and particle kernels' arguments
+    return LBM_OK;
+}
+
+int lbm_record_force(lbm_handle* h, int32_t id, int32_t on) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    BIND(h);
+    if (id < 1 || id > (int)h->hparts.size()) return set_err(h, LBM_ERR_INVALID, "no such particle");
+    const int v = on ? 1 : 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&h->d_parts[id - 1].recordF, &v, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
 }
 
 int lbm_get_mask(lbm_handle* h, int32_t id, uint8_t* mask) {
@@ -1760,6 +2140,7 @@ int lbm_step_noalloc(lbm_handle* h, int64_t nsteps) {
         launch_bulk(h, a, h->stream);
         if (nb > 0) h->ops.fixup(a, (unsigned)fixup_grid(h), h->stream, false, fixup_walk(h));
         if (np > 0) {
+            launch_interactions(h, h->stream);
             h->ops.particles(pa, (unsigned)np, h->stream);
             h->ops.links(pa, np, h->link_bpp, h->d_linkcnt, h->stream);
         }
@@ -1953,7 +2334,7 @@ void batch_launch(lbm_batch* b, int s, const TickItems& it, int q, cudaStream_t 
     const unsigned grid = (unsigned)std::max<long long>(1, std::min(items, cap));
     const size_t n = b->reps.size();
     b->ops.tick(b->d_targs + (size_t)s * n, b->d_pargs + (size_t)s * n, it, b->d_tq + q,
-                b->d_err + n, grid, st);
+                b->d_err + n, grid, st, b->reps[0]->rounding == LBM_ROUND_STOCHASTIC);
 }
 
 // one tick of every replica with arguments of parity s (capturable)
@@ -1965,7 +2346,8 @@ void batch_enqueue(lbm_batch* b, int s) {
     // stream order: all tiles; then the fix-up blocks once the previous
     // particle update is done; the particle update on the side stream
     if (b->tuning.tile_cta)
-        b->ops.bulk_batch(b->d_targs + (size_t)s * b->reps.size(), b->d_dmap, b->nd, b->stream);
+        b->ops.bulk_batch(b->d_targs + (size_t)s * b->reps.size(), b->d_dmap, b->nd, b->stream,
+                          b->reps[0]->rounding == LBM_ROUND_STOCHASTIC);
     else
         batch_launch(b, s, batch_items(b, false, false, false, true, 0), 0, b->stream);
     if (b->part_pending) {
@@ -2131,6 +2513,7 @@ int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticle
             batch_destroy_all(b);
             return bset_err(nullptr, rc, m);
         }
+        h->in_batch = true;
         b->reps.push_back(h);
         const int np = nparticles ? nparticles[r] : 0;
         for (int p = 0; p < np; ++p, ++k) {
@@ -2145,8 +2528,9 @@ int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticle
         std::string why;
         if (!use_vector_bulk(h) || h->vblock != kTickBlock || !h->ops.tick) why = "needs the vector bulk path with x-rows of at most 256 nodes";
         else if (h->device != h0->device) why = "all replicas must be on one device";
-        else if (h->lattice != h0->lattice || h->storage != h0->storage || h->trt != h0->trt)
-            why = "all replicas must share the velocity set, storage format and collision model";
+        else if (h->lattice != h0->lattice || h->storage != h0->storage || h->trt != h0->trt ||
+                 h->rounding != h0->rounding)
+            why = "all replicas must share the velocity set, storage format, rounding and collision model";
         if (!why.empty()) {
             batch_destroy_all(b);
             return bset_err(nullptr, LBM_ERR_UNSUPPORTED, "replica " + std::to_string(r) + ": " + why);
@@ -2171,7 +2555,9 @@ int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticle
     if (!rc && (cudaMemset(b->d_tq, 0, sizeof(TickCounters) * 2) != cudaSuccess ||
                 cudaMemset(b->d_err, 0, sizeof(int) * (n + 1)) != cudaSuccess))
         rc = bset_err(b, LBM_ERR_CUDA, "memset failed");
-    if (!rc && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->max_per_sm, b->ops.tick_fn, kTickBlock, 0) != cudaSuccess ||
+    if (!rc && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &b->max_per_sm, b->reps[0]->rounding == LBM_ROUND_STOCHASTIC ? b->ops.tick_fn_sr : b->ops.tick_fn,
+                    kTickBlock, 0) != cudaSuccess ||
                 cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess))
         rc = bset_err(b, LBM_ERR_CUDA, "occupancy query failed");
     if (rc) {
@@ -2199,6 +2585,8 @@ int lbm_batch_step(lbm_batch* b, int64_t nsteps) {
         if (cudaStreamSynchronize(h->stream) != cudaSuccess)
             return bset_err(b, LBM_ERR_CUDA, "replica stream failed");
     }
+    for (lbm_handle* h : b->reps)
+        if (!h->inter.empty()) return bset_err(b, LBM_ERR_UNSUPPORTED, "batches do not run particle interactions");
     int rc = batch_prepare(b);
     if (rc) return rc;
     if (b->profiling) BCUDA_TRY(b, cudaEventRecord(b->t_begin, b->stream));
@@ -2521,11 +2909,11 @@ int backward_tick(AdjointRun& R, long long n) {
     const ParticleDev& P1 = R.rec[n + 1];
     PartAdj& A = R.pa;
     const double dt = h->dt;
-    // the observable reads the velocity after tick n + 1
-    if (n + 1 >= R.spec.window_begin && n + 1 <= R.spec.window_end) {
-        const double K = (double)(R.spec.window_end - R.spec.window_begin + 1);
+    // the observable reads the velocity after tick n + 1, or the force of tick n + 1
+    const bool in_window = n + 1 >= R.spec.window_begin && n + 1 <= R.spec.window_end;
+    const double K = (double)(R.spec.window_end - R.spec.window_begin + 1);
+    if (in_window && R.spec.observable == LBM_OBSERVABLE_VELOCITY)
         for (int k = 0; k < D; ++k) A.v[k] += R.e0[k] / K;
-    }
     // reverse the particle update of tick n (particles.cuh, moveParticles!)
     bool moved = false, alpha = false;
     if (P0.coupleF)
@@ -2571,6 +2959,8 @@ int backward_tick(AdjointRun& R, long long n) {
         for (int k = 0; k < D; ++k) A.v[k] += dt * A.R[k];                                    // R' = R + dt v'
         for (int k = 0; k < D; ++k) a.lamF[k] = dt * P0.inv_mass * A.v[k];                   // v' = v + dt F / m
     }
+    if (in_window && R.spec.observable == LBM_OBSERVABLE_FORCE)
+        for (int k = 0; k < D; ++k) a.lamF[k] += R.e0[k] / K;  // J += e.F / K
     // the field adjoint of tick n on the device
     a.src = h->pop[h->cur];
     a.lam_in = R.lam[R.lcur];
@@ -2680,6 +3070,9 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
     BIND(h);
     const auto t0 = std::chrono::steady_clock::now();
     if (h->hparts.size() != 1) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint supports models with one particle");
+    if (h->particle_rules != LBM_RULES_GPU_MODULE)
+        return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint follows the GPU module's particle update");
+    if (!h->inter.empty()) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support particle interactions");
     if (h->has_walls) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support walls");
     if (h->force_mode == LBM_FORCE_FIELD) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support force fields");
     if (spec->ticks < 1 || spec->window_begin < 1 || spec->window_end < spec->window_begin ||
@@ -2696,6 +3089,13 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
     R.have[0] = 1;
     join_particles(h);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (spec->observable != LBM_OBSERVABLE_VELOCITY && spec->observable != LBM_OBSERVABLE_FORCE)
+        return set_err(h, LBM_ERR_INVALID, "unknown observable");
+    const int record = spec->observable == LBM_OBSERVABLE_FORCE ? 1 : 0;
+    int record_before = 0;  // the caller's lbm_record_force setting, restored at the end
+    CUDA_TRY(h, cudaMemcpy(&record_before, &h->d_parts[0].recordF, sizeof(int), cudaMemcpyDeviceToHost));
+    // the force observable needs the momentum exchange even of a held particle
+    CUDA_TRY(h, cudaMemcpy(&h->d_parts[0].recordF, &record, sizeof(int), cudaMemcpyHostToDevice));
     CUDA_TRY(h, cudaMemcpy(&R.rec[0], h->d_parts, sizeof(ParticleDev), cudaMemcpyDeviceToHost));
     double en = 0.0;
     for (int k = 0; k < 3; ++k) en += spec->direction[k] * spec->direction[k];
@@ -2736,6 +3136,9 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
         }
     }
     while (!R.snaps.empty()) snap_pop(R);
+    if (cudaMemcpy(&h->d_parts[0].recordF, &record_before, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess &&
+        !rc)
+        rc = set_err(h, LBM_ERR_CUDA, "cannot restore the force record flag");
     dev_free(R.lam[0]);
     dev_free(R.lam[1]);
     dev_free(R.partial);
@@ -2746,7 +3149,8 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
     const double K = (double)(spec->window_end - spec->window_begin + 1);
     double J = 0.0;
     for (long long t = spec->window_begin; t <= spec->window_end; ++t)
-        for (int k = 0; k < h->dims; ++k) J += R.rec[t].v[k] * R.e0[k] / K;
+        for (int k = 0; k < h->dims; ++k)
+            J += (record ? R.rec[t].lastF[k] : R.rec[t].v[k]) * R.e0[k] / K;
     out->value = J;
     out->dB1 = R.dB1;
     out->dB2 = R.dB2;

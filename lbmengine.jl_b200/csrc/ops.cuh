@@ -24,6 +24,7 @@ struct Ops {
     void (*encode)(const CodecArgs&, cudaStream_t);
     void (*decode)(const CodecArgs&, cudaStream_t);
     void (*macro)(const CodecArgs&, cudaStream_t);
+    void (*stress)(const CodecArgs&, cudaStream_t);
     void (*check)(const CodecArgs&, int*, cudaStream_t);
     void (*init)(const InitArgs&, cudaStream_t);
     void (*mask)(const MaskArgs&, cudaStream_t);
@@ -31,21 +32,24 @@ struct Ops {
     void (*bulk_v4)(const StepArgs&, long long tiles, int block, cudaStream_t);
     // the same pass with TMA bulk loads through a shared-memory ring (bulk_tma.cuh); null for FP64
     void (*bulk_tma)(const StepArgs&, const TmaShape&, cudaStream_t);
-    // one persistent kernel per tick over the A/B/C/D item queue (tick.cuh)
+    // one persistent kernel per tick over the A/B/C/D item queue (tick.cuh);
+    // sr: the 2-byte stores round stochastically
     void (*tick)(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
-                 int* err, unsigned grid, cudaStream_t);
+                 int* err, unsigned grid, cudaStream_t, bool sr);
     // a batch's bulk tiles, one CTA per entry of dmap
-    void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t);
+    void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t, bool sr);
     // discrete adjoint of one tick, and of the initial condition (adjoint.cuh)
     void (*adjoint)(const AdjArgs&, cudaStream_t);
     void (*adjoint_init)(const AdjArgs&, cudaStream_t);
     const void* bulk_fn;      // kernel symbols (occupancy queries, attributes)
     const void* bulk_tma_fn;
     const void* fixup_fn;
-    const void* tick_fn;
+    const void* tick_fn;      // the round-to-nearest variants (occupancy queries)
+    const void* tick_fn_sr;   // the stochastic-rounding variant
+    const void* bulk_tma_fn_sr;
 };
 
-constexpr int kBulkBlocks[4] = {64, 128, 256, 512};  // CTA sizes of the vector bulk kernel
+constexpr int kBulkBlocks[4] = {64, 128, 256, 512};  // CTA sizes of the vector bulk kernel (and 32 on request)
 
 inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
@@ -75,26 +79,54 @@ struct OpsImpl {
         k_links_count<L><<<(unsigned)(nparts * bpp), kLinkBlock, 0, s>>>(a, bpp, counts);
         k_links_write<L><<<(unsigned)(nparts * bpp), kLinkBlock, 0, s>>>(a, bpp, counts);
     }
+    static constexpr bool kTwo = Store<ST>::bytes == 2;  // stochastic variants exist for 2-byte storage
+    template <bool SR>
+    static void bulk_v4_sr(const StepArgs& a, long long tiles, int block, cudaStream_t s) {
+        const unsigned g = (unsigned)tiles;
+        if (block <= 32) k_bulk_v4<L, ST, TRT, 32, SR><<<g, 32, 0, s>>>(a);
+        else if (block <= 64) k_bulk_v4<L, ST, TRT, 64, SR><<<g, 64, 0, s>>>(a);
+        else if (block <= 128) k_bulk_v4<L, ST, TRT, 128, SR><<<g, 128, 0, s>>>(a);
+        else if (block <= 256) k_bulk_v4<L, ST, TRT, 256, SR><<<g, 256, 0, s>>>(a);
+        else k_bulk_v4<L, ST, TRT, 512, SR><<<g, 512, 0, s>>>(a);
+    }
     static void bulk_v4(const StepArgs& a, long long tiles, int block, cudaStream_t s) {
         if constexpr (ST != ST_F64) {
-            const unsigned g = (unsigned)tiles;
-            if (block <= 64) k_bulk_v4<L, ST, TRT, 64><<<g, 64, 0, s>>>(a);
-            else if (block <= 128) k_bulk_v4<L, ST, TRT, 128><<<g, 128, 0, s>>>(a);
-            else if (block <= 256) k_bulk_v4<L, ST, TRT, 256><<<g, 256, 0, s>>>(a);
-            else k_bulk_v4<L, ST, TRT, 512><<<g, 512, 0, s>>>(a);
+            if constexpr (kTwo)
+                if (a.stochastic) return bulk_v4_sr<true>(a, tiles, block, s);
+            bulk_v4_sr<false>(a, tiles, block, s);
         }
     }
     static void bulk_tma(const StepArgs& a, const TmaShape& sh, cudaStream_t s) {
-        if constexpr (ST != ST_F64)
-            k_bulk_tma<L, ST, TRT><<<(unsigned)sh.grid, (unsigned)(sh.rows * (a.g.n[0] / 4)), (size_t)sh.smem, s>>>(
-                a, sh.rows, sh.stages);
+        if constexpr (ST != ST_F64) {
+            const dim3 g((unsigned)sh.grid), b((unsigned)(sh.rows * (a.g.n[0] / 4)));
+            if constexpr (kTwo)
+                if (a.stochastic) {
+                    k_bulk_tma<L, ST, TRT, true><<<g, b, (size_t)sh.smem, s>>>(a, sh.rows, sh.stages);
+                    return;
+                }
+            k_bulk_tma<L, ST, TRT, false><<<g, b, (size_t)sh.smem, s>>>(a, sh.rows, sh.stages);
+        }
     }
     static void tick(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
-                     int* err, unsigned grid, cudaStream_t s) {
-        if constexpr (ST != ST_F64) k_tick<L, ST, TRT><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
+                     int* err, unsigned grid, cudaStream_t s, bool sr) {
+        if constexpr (ST != ST_F64) {
+            if constexpr (kTwo)
+                if (sr) {
+                    k_tick<L, ST, TRT, true><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
+                    return;
+                }
+            k_tick<L, ST, TRT, false><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
+        }
     }
-    static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s) {
-        if constexpr (ST != ST_F64) k_bulk_batch<L, ST, TRT><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+    static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s, bool sr) {
+        if constexpr (ST != ST_F64) {
+            if constexpr (kTwo)
+                if (sr) {
+                    k_bulk_batch<L, ST, TRT, true><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+                    return;
+                }
+            k_bulk_batch<L, ST, TRT, false><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+        }
     }
     static void adjoint(const AdjArgs& a, cudaStream_t s) {
         k_adjoint<L, ST, TRT><<<blocks_for(a.g.N, kAdjBlock), kAdjBlock, 0, s>>>(a);
@@ -105,6 +137,7 @@ struct OpsImpl {
     static void encode(const CodecArgs& a, cudaStream_t s) { k_encode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void macro(const CodecArgs& a, cudaStream_t s) { k_macro<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
+    static void stress(const CodecArgs& a, cudaStream_t s) { k_stress<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void check(const CodecArgs& a, int* bad, cudaStream_t s) {
         k_check<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a, bad);
     }
@@ -119,21 +152,28 @@ struct OpsImpl {
         o.encode = encode;
         o.decode = decode;
         o.macro = macro;
+        o.stress = stress;
         o.check = check;
         o.init = init;
         o.mask = mask;
         o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;
         o.bulk_tma = ST == ST_F64 ? nullptr : bulk_tma;
-        o.bulk_tma_fn = nullptr;
-        if constexpr (ST != ST_F64) o.bulk_tma_fn = (const void*)k_bulk_tma<L, ST, TRT>;
+        o.bulk_tma_fn = o.bulk_tma_fn_sr = nullptr;
+        if constexpr (ST != ST_F64) {
+            o.bulk_tma_fn = (const void*)k_bulk_tma<L, ST, TRT, false>;
+            o.bulk_tma_fn_sr = kTwo ? (const void*)k_bulk_tma<L, ST, TRT, kTwo> : o.bulk_tma_fn;
+        }
         o.tick = ST == ST_F64 ? nullptr : tick;
         o.bulk_batch = ST == ST_F64 ? nullptr : bulk_batch;
         o.adjoint = adjoint;
         o.adjoint_init = adjoint_init;
         o.bulk_fn = (const void*)k_bulk<L, ST, TRT>;
         o.fixup_fn = (const void*)k_fixup<L, ST, TRT>;
-        o.tick_fn = nullptr;
-        if constexpr (ST != ST_F64) o.tick_fn = (const void*)k_tick<L, ST, TRT>;
+        o.tick_fn = o.tick_fn_sr = nullptr;
+        if constexpr (ST != ST_F64) {
+            o.tick_fn = (const void*)k_tick<L, ST, TRT, false>;
+            o.tick_fn_sr = kTwo ? (const void*)k_tick<L, ST, TRT, kTwo> : o.tick_fn;
+        }
         return o;
     }
 };

@@ -41,6 +41,10 @@ struct ParticleArgs {
     int pad;
     int* nbox_out[2];  // [nparts][6] solid boxes (lo, hi) published for the bulk pass two ticks
                        // later (tick update writes [0]; setup writes both); null to skip
+    double* trj;       // trajectory ring: [trj_cap][nparts][9] (position, velocity, angular
+                       // velocity after each tick's update), or null
+    long long trj_cap;
+    const double* fint;  // [nparts][3] forces of the particle interactions (interactions.cuh), or null
 };
 
 // publish particle p's solid box for the far/near split of the bulk pass
@@ -245,9 +249,24 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             }
         }
         const double dt = a.dt;
+        if (a.mode == 0 && a.fint)  // molecularDynamicsTick!: the interactions' share of the force input
+            for (int k = 0; k < 3; ++k) F[k] += a.fint[3 * p + k];
+        const bool cpu = P.rules == 1;  // LBM_RULES_CPU_MODULE
         if (tid == 0) {
             bool moved = a.mode != 0;
-            if (a.mode == 0 && P.coupleF) {
+            if (a.mode == 0 && cpu) {
+                // src/cpu/particles.jl:55-60: v += m^-1 dP (dP = dt F, the momentum
+                // input of the tick), then an Euler step whenever v != 0
+                bool vnz = false;
+                for (int k = 0; k < D; ++k) {
+                    P.v[k] = P.v[k] + P.inv_mass * (dt * F[k]);
+                    vnz = vnz || P.v[k] != 0.0;
+                }
+                if (vnz) {
+                    for (int k = 0; k < D; ++k) P.R[k] = P.R[k] + dt * P.v[k];
+                    moved = true;
+                }
+            } else if (a.mode == 0 && P.coupleF) {
                 for (int k = 0; k < D; ++k) P.v[k] = P.v[k] + dt * (F[k] * P.inv_mass);
                 for (int k = 0; k < D; ++k) P.R[k] = P.R[k] + dt * P.v[k];
                 for (int k = 0; k < D; ++k)
@@ -255,10 +274,21 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
             }
             s_moved = moved ? 1 : 0;
             if (a.mode != 2)
-                for (int k = 0; k < 3; ++k) {
-                    P.lastF[k] = F[k];
-                    P.lastT[k] = T[k];
+                for (int k = 0; k < 3; ++k) {  // CPU rules report the momentum inputs dP, dL
+                    P.lastF[k] = cpu ? dt * F[k] : F[k];
+                    P.lastT[k] = cpu ? dt * T[k] : T[k];
                 }
+        } else if (cpu) {  // w += I^-1 dL; the swimming direction never rotates (:7-18)
+            bool alpha = false;
+            if (a.mode == 0) {
+                const int nw2 = D == 2 ? 1 : 3;
+                for (int k = 0; k < nw2; ++k) {
+                    const double dL = dt * T[k];
+                    P.w[k] = P.w[k] + P.inv_inertia * dL;
+                    alpha = alpha || dL != 0.0;
+                }
+            }
+            s_alpha = alpha ? 1 : 0;
         } else {
             bool alpha = false;
             if (a.mode == 0 && P.coupleT) {
@@ -310,6 +340,15 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a, const int 
                 P.sE[k] = P.e[k];
             }
         s_moved = moved ? 1 : 0;
+        if (a.mode == 0 && a.trj) {  // the state writeParticleTrajectory writes after each tick
+            double* r = a.trj + ((P.nrec % a.trj_cap) * a.nparts + p) * 9;
+            for (int k = 0; k < 3; ++k) {
+                r[k] = P.R[k];
+                r[3 + k] = P.v[k];
+                r[6 + k] = P.w[k];
+            }
+            P.nrec += 1;
+        }
         s_changed = (a.mode != 0 || !P.valid) ? 1 : 0;
         s_bad = 0;
         s_nonempty = 0;

@@ -39,6 +39,53 @@ __device__ __forceinline__ float round_dither(float v, unsigned key, unsigned mu
     return __uint_as_float((b + (h >> (32 - DROP))) & M);
 }
 
+// Dither of a thread's group of four cells (the vector bulk kernels): one
+// well-mixed 32-bit word from the group's first cell and the kept bits of
+// three of its post-collision values (which change from tick to tick as the
+// flow evolves), spread into four independent words (dither_words).  The
+// value of direction i of cell k adds word (k + i) mod 4 to its FP32 bits and
+// is converted rounding toward zero: the discarded fraction is rounded up
+// exactly when it exceeds the dither.  For every (k, i) the dither is uniform
+// over the nodes of a flow, so the rounding is unbiased, at one integer
+// addition per value.
+__device__ __forceinline__ unsigned group_dither(int cell0, float v1, float v2, float v3) {
+    unsigned x = ((__float_as_uint(v1) ^ __float_as_uint(v2) ^ __float_as_uint(v3)) & 0xFFFFE000u) ^
+                 ((unsigned)cell0 * kDitherCell);
+    x *= 0x9E3779B1u;
+    x ^= x >> 15;
+    x *= 0x2C1B3C6Du;
+    x ^= x >> 13;
+    return x;
+}
+
+// four independent dither words of DROP bits from a group's word
+template <int DROP>
+__device__ __forceinline__ void dither_words(unsigned x, unsigned* w) {
+    unsigned y = x * 0x85EBCA6Bu;
+    y ^= y >> 13;
+    constexpr unsigned M = (1u << DROP) - 1u;
+    w[0] = x & M;
+    w[1] = (x >> 16) & M;
+    w[2] = y & M;
+    w[3] = (y >> 16) & M;
+}
+
+// v with a dither added to its bits below the kept ones (a conversion toward
+// zero then rounds it stochastically)
+__device__ __forceinline__ float add_dither(float v, unsigned d) { return __uint_as_float(__float_as_uint(v) + d); }
+
+// two floats to a packed half2 / bfloat162 rounding toward zero (lo in the low half)
+__device__ __forceinline__ unsigned pack_half2_rz(float lo, float hi) {
+    unsigned r;
+    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ unsigned pack_bf162_rz(float lo, float hi) {
+    unsigned r;
+    asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 enum StoreKind { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2, ST_F64 = 3 };
 
 template <int S> struct Store;
@@ -50,6 +97,7 @@ template <> struct Store<ST_F32> {
     static __device__ __forceinline__ T enc(R v, R) { return v; }
     static __device__ __forceinline__ T enc_sr(R v, R, unsigned, int) { return v; }
     static constexpr int bytes = 4;
+    static constexpr int drop = 0;
 };
 template <> struct Store<ST_F64> {
     using T = double;
@@ -58,6 +106,7 @@ template <> struct Store<ST_F64> {
     static __device__ __forceinline__ T enc(R v, R) { return v; }
     static __device__ __forceinline__ T enc_sr(R v, R, unsigned, int) { return v; }
     static constexpr int bytes = 8;
+    static constexpr int drop = 0;
 };
 template <> struct Store<ST_F16> {
     using T = __half;
@@ -69,6 +118,7 @@ template <> struct Store<ST_F16> {
         return __float2half_rn(round_dither<13>(v * scale, (cell & ~3u) * kDitherCell, dither_mul(dir, cell & 3u)));
     }
     static constexpr int bytes = 2;
+    static constexpr int drop = 13;  // FP32 mantissa bits below an IEEE half's
 };
 template <> struct Store<ST_BF16> {
     using T = __nv_bfloat16;
@@ -80,6 +130,7 @@ template <> struct Store<ST_BF16> {
             round_dither<16>(v * scale, (cell & ~3u) * kDitherCell, dither_mul(dir, cell & 3u)));
     }
     static constexpr int bytes = 2;
+    static constexpr int drop = 16;  // FP32 mantissa bits below a bfloat16's
 };
 
 }  // namespace lbm

@@ -124,7 +124,7 @@ __device__ __forceinline__ long long near_slot_tile(const StepArgs& a, int p, in
     return ty + (long long)a.vnt1 * tz;
 }
 
-template <class L, int ST, bool TRT>
+template <class L, int ST, bool TRT, bool SR>
 __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restrict__ args,
                                                        const ParticleArgs* __restrict__ pargs, const TickItems it,
                                                        TickCounters* q, int* err) {
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
             const StepArgs& A = args[m.x];
             const long long tile =
                 m.y == 0 ? (long long)m.z : near_slot_tile<L::D>(A, m.z, m.w & 0xffff, m.w >> 16);
-            if (tile >= 0) bulk_v4_tile<L, ST, TRT, B>(A, tile, s_ex);
+            if (tile >= 0) bulk_v4_tile<L, ST, TRT, B, SR>(A, tile, s_ex);
             cta_done(&q->cnt_a);
         } else if (t < nab) {
             cta_wait(&q->cnt_a, (int)it.na + it.wait_extra, err, it.spin_limit);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
                 for (int p = threadIdx.x; p < A.nparts; p += B) nr = nr || tile_meets_box<L::D>(A, m.y, p);
                 skip = __syncthreads_or(nr);
             }
-            if (!skip) bulk_v4_tile<L, ST, TRT, B>(A, m.y, s_ex);
+            if (!skip) bulk_v4_tile<L, ST, TRT, B, SR>(A, m.y, s_ex);
         }
         if (threadIdx.x == 0) s_next = nxt;
         __syncthreads();
@@ -185,12 +185,12 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
 
 // The bulk tiles of a batch, one CTA per item of the D map (no queue): the
 // replicas' arguments come from `args[dmap[i].x]`.
-template <class L, int ST, bool TRT>
-__global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L, ST>() / kTickBlock)
+template <class L, int ST, bool TRT, bool SR>
+__global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L, ST, SR>() / kTickBlock)
     k_bulk_batch(const StepArgs* __restrict__ args, const int2* __restrict__ dmap) {
     __shared__ float s_ex[x_moving_dirs<L>()][kTickBlock];
     const int2 m = dmap[blockIdx.x];
-    bulk_v4_tile<L, ST, TRT, kTickBlock>(args[m.x], m.y, s_ex);
+    bulk_v4_tile<L, ST, TRT, kTickBlock, SR>(args[m.x], m.y, s_ex);
 }
 
 }  // namespace lbm

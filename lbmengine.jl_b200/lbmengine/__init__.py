@@ -10,9 +10,12 @@ The compute path is liblbm_b200.so (CUDA, sm_100a), loaded through ctypes.
 """
 from .config import DEFAULT, julia_float_range, resolve_bead, resolve_model, resolve_squirmer  # noqa: F401
 from .model import (LBMmodel, LBMparticle, LBMpropagate, addBead, addSquirmer,  # noqa: F401
-                    hydroVariablesUpdate, modelInit)
+                    hydroVariablesUpdate, modelInit, viscousStressTensor)
+from .interactions import (addBistableBond, addDipoles, addLennardJones, addLinearBond,  # noqa: F401
+                           addPolarBond, addWCA)
 from .batch import LBMbatch  # noqa: F401
 from . import _capi  # noqa: F401
 
 __all__ = ["modelInit", "addSquirmer", "addBead", "LBMpropagate", "hydroVariablesUpdate", "LBMmodel",
-           "LBMparticle", "LBMbatch", "DEFAULT"]
+           "LBMparticle", "LBMbatch", "DEFAULT", "viscousStressTensor", "addLinearBond", "addPolarBond",
+           "addBistableBond", "addDipoles", "addLennardJones", "addWCA"]

@@ -30,6 +30,11 @@ LBM_SCHEDULE_AUTO, LBM_SCHEDULE_STREAM, LBM_SCHEDULE_PERSISTENT = 0, 1, 3
 SCHEDULE_NAMES = {"auto": LBM_SCHEDULE_AUTO, "stream": LBM_SCHEDULE_STREAM, "persistent": LBM_SCHEDULE_PERSISTENT}
 LBM_RULES_GPU_MODULE, LBM_RULES_CPU_MODULE = 0, 1
 LBM_BULK_AUTO, LBM_BULK_VECTOR, LBM_BULK_TMA, LBM_BULK_SCALAR = 0, 1, 2, 3
+LBM_OBSERVABLE_VELOCITY, LBM_OBSERVABLE_FORCE = 0, 1
+LBM_ROUND_STOCHASTIC, LBM_ROUND_NEAREST = 0, 1
+(LBM_INTERACTION_LINEAR, LBM_INTERACTION_BISTABLE, LBM_INTERACTION_POLAR, LBM_INTERACTION_LENNARD_JONES,
+ LBM_INTERACTION_DIPOLE) = range(5)
+ROUNDING_NAMES = {"stochastic": LBM_ROUND_STOCHASTIC, "nearest": LBM_ROUND_NEAREST}
 RULES_NAMES = {"gpu": LBM_RULES_GPU_MODULE, "cpu": LBM_RULES_CPU_MODULE}
 
 _dp = C.POINTER(C.c_double)
@@ -63,7 +68,7 @@ class LbmConfig(C.Structure):
         ("device", C.c_int32),
         ("schedule", C.c_int32),
         ("particle_rules", C.c_int32),
-        ("reserved", C.c_int32),
+        ("rounding", C.c_int32),
     ]
 
 
@@ -124,6 +129,16 @@ class LbmInfo(C.Structure):
     ]
 
 
+class LbmInteraction(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("id1", C.c_int32),
+        ("id2", C.c_int32),
+        ("id3", C.c_int32),
+        ("p", C.c_double * 4),
+    ]
+
+
 class LbmProfile(C.Structure):
     _fields_ = [
         ("total_ms", C.c_double),
@@ -156,7 +171,7 @@ class LbmAdjointSpec(C.Structure):
         ("direction", C.c_double * 3),
         ("tau_minus_slope", C.c_double),
         ("snapshots", C.c_int32),
-        ("reserved", C.c_int32),
+        ("observable", C.c_int32),
     ]
 
 
@@ -185,10 +200,17 @@ PROTOTYPES = [
     ("lbm_step", C.c_int, [C.c_void_p, C.c_int64]),
     ("lbm_get_fields", C.c_int, [C.c_void_p, _dp, _dp]),
     ("lbm_get_distributions", C.c_int, [C.c_void_p, _dp]),
+    ("lbm_get_stress", C.c_int, [C.c_void_p, _dp]),
+    ("lbm_record_trajectories", C.c_int, [C.c_void_p, C.c_int64]),
+    ("lbm_read_trajectories", C.c_int, [C.c_void_p, _dp, C.c_int64, C.POINTER(C.c_int64)]),
+    ("lbm_write_fluid_csv", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("lbm_output_flush", C.c_int, [C.c_void_p]),
     ("lbm_set_distributions", C.c_int, [C.c_void_p, _dp]),
     ("lbm_get_particles", C.c_int, [C.c_void_p, C.POINTER(LbmParticleState), C.c_int32, C.POINTER(C.c_int32)]),
     ("lbm_set_particle", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(LbmParticleState)]),
     ("lbm_get_mask", C.c_int, [C.c_void_p, C.c_int32, _u8p]),
+    ("lbm_record_force", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    ("lbm_set_interactions", C.c_int, [C.c_void_p, C.POINTER(LbmInteraction), C.c_int32]),
     ("lbm_get_links", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.c_int64,
                                 C.POINTER(C.c_int64)]),
     ("lbm_get_info", C.c_int, [C.c_void_p, C.POINTER(LbmInfo)]),

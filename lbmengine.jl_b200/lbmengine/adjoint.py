@@ -32,13 +32,15 @@ def tau_minus_slope(resolved) -> float:
     return -float(lam) * dt * dt / (resolved.tau - dt / 2) ** 2
 
 
-def swimming_speed_gradient(model: mdl.LBMmodel, ticks: int, window, direction=None, snapshots: int = 32):
+def swimming_speed_gradient(model: mdl.LBMmodel, ticks: int, window, direction=None, snapshots: int = 32,
+                            observable: int = capi.LBM_OBSERVABLE_VELOCITY):
     """Average over ticks window[0]..window[1] of the particle velocity along
     ``direction`` (default: its initial swimming direction), over ``ticks``
     ticks from the model's initial state, and its gradient.  The model is left
     as it was."""
     spec = capi.LbmAdjointSpec(ticks=int(ticks), window_begin=int(window[0]), window_end=int(window[1]),
-                               tau_minus_slope=tau_minus_slope(model._res), snapshots=int(snapshots))
+                               tau_minus_slope=tau_minus_slope(model._res), snapshots=int(snapshots),
+                               observable=int(observable))
     if direction is not None:
         for k, v in enumerate(direction):
             spec.direction[k] = float(v)
@@ -47,6 +49,14 @@ def swimming_speed_gradient(model: mdl.LBMmodel, ticks: int, window, direction=N
     grad = dict(B1=res.dB1, B2=res.dB2, tau=res.dtau, Fx=res.dF[0], Fy=res.dF[1], Fz=res.dF[2])
     return SimpleNamespace(value=res.value, grad=grad, dtau_plus=res.dtau_plus, dtau_minus=res.dtau_minus,
                            forward_ticks=res.forward_ticks, snapshots_used=res.snapshots_used, ms=res.ms)
+
+
+def drag_gradient(model: mdl.LBMmodel, ticks: int, window, direction=None, snapshots: int = 32):
+    """Average over ticks window[0]..window[1] of the momentum-exchange force on
+    the particle along ``direction`` (default: its initial swimming direction)
+    and its gradient; for a held particle (coupleForces false) this is its
+    drag.  The model is left as it was."""
+    return swimming_speed_gradient(model, ticks, window, direction, snapshots, capi.LBM_OBSERVABLE_FORCE)
 
 
 def build_swimmer(model_kw: dict, squirmer_kw: dict, theta=None) -> mdl.LBMmodel:

@@ -102,7 +102,7 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
                   walledDimensions=DEFAULT, dampenEcho=False, walls=DEFAULT, movingWalls=DEFAULT,
                   isFluidCompressible=True, forceDensity=DEFAULT, forcingScheme=DEFAULT, saveData=False,
                   storage="f32", rho_ref=DEFAULT, store_scale=DEFAULT, device=DEFAULT, schedule="auto",
-                  particleRules="gpu"):
+                  particleRules="gpu", rounding="stochastic"):
     """Resolve modelInit's keywords (src/gpu/initMethods.jl:440-702) into an LbmConfig.
 
     Returns a namespace with ``cfg`` (capi.LbmConfig), ``keep`` (arrays the
@@ -191,8 +191,8 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
         else:
             raise ValueError("force density does not have consistent dimensions!")
         schemes.append(fsch)
-    if saveData:
-        raise NotImplementedError("saveData (CSV trajectory output) is not part of the time-step library")
+    if saveData:  # initMethods.jl:671-675: the output directory is made by the front end
+        schemes.append("saveData")
     cfg = capi.LbmConfig()
     cfg.dims = dims
     cfg.lattice = lattice
@@ -253,6 +253,10 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
     if particleRules not in capi.RULES_NAMES:
         raise ValueError(f"particleRules must be one of {sorted(capi.RULES_NAMES)}")
     cfg.particle_rules = capi.RULES_NAMES[particleRules]
+    # rounding of the F16/BF16 stores: "stochastic" (unbiased, the default) or "nearest"
+    if rounding not in capi.ROUNDING_NAMES:
+        raise ValueError(f"rounding must be one of {sorted(capi.ROUNDING_NAMES)}")
+    cfg.rounding = capi.ROUNDING_NAMES[rounding]
     return SimpleNamespace(cfg=cfg, keep=keep, dt=dt, tau=tau, tau_minus=tau_minus, viscosity=nu,
                            relaxationTimeRatio=ratio, coordinates=axes, shape=shape, dims=dims,
                            velocities=vname, collision=cm, schemes=list(dict.fromkeys(schemes)),

@@ -15,6 +15,8 @@ import numpy as np
 
 from . import _capi as capi
 from . import config as cfgmod
+from . import interactions
+from . import output
 from .config import DEFAULT
 
 
@@ -49,6 +51,10 @@ class LBMmodel:
         info = self.info()
         self._q = info.q
         self._cells = info.cells
+        if self._owned and "saveData" in self.schemes:  # modelInit: fresh output.lbm, the initial fluid
+            output.prepare_directory()
+            output.write_fluid(self)
+            self._check(self._lib.lbm_output_flush(self._h))
 
     # ---- handle plumbing -------------------------------------------------
     def _check(self, code):
@@ -113,6 +119,13 @@ class LBMmodel:
         flat = np.ascontiguousarray(f.ravel(order="F"))
         self._check(self._lib.lbm_set_distributions(self._h, flat.ctypes.data_as(capi._dp)))
 
+    def viscous_stress_tensor(self) -> np.ndarray:
+        """viscousStressTensor(model) (src/cpu/fluids.jl:507-520): array (N..., d, d)."""
+        d = self._dims
+        s = np.empty(self._cells * d * d, dtype=np.float64)
+        self._check(self._lib.lbm_get_stress(self._h, s.ctypes.data_as(capi._dp)))
+        return s.reshape(self._shape + (d, d), order="F")
+
     def particle_states(self):
         cnt = C.c_int32()
         self._check(self._lib.lbm_get_particles(self._h, None, 0, C.byref(cnt)))
@@ -160,6 +173,11 @@ class LBMmodel:
     def step(self, n: int) -> None:
         self._check(self._lib.lbm_step(self._h, int(n)))
 
+    def record_force(self, pid: int, on: bool = True) -> None:
+        """Report the momentum-exchange force of particle pid even when it is held
+        (coupleForces false), without applying it: its drag (lbm_record_force)."""
+        self._check(self._lib.lbm_record_force(self._h, int(pid), int(bool(on))))
+
     def save_state(self, path: str) -> None:
         self._check(self._lib.lbm_save_state(self._h, path.encode()))
 
@@ -184,11 +202,16 @@ def _add(model: LBMmodel, params) -> int:
     for s in ("ladd", "bounceBack"):
         if s not in model.schemes:
             model.schemes.append(s)
+    if "saveData" in model.schemes:  # writeParticleTrajectory of the new particle (initMethods.jl:86, 219)
+        output.write_particle(model, model.particle_states()[pid.value - 1])
     return pid.value
 
 
 def addSquirmer(model: LBMmodel, **kw) -> None:
-    """addSquirmer!(model; ...) — src/gpu/initMethods.jl:91-222."""
+    """addSquirmer!(model; ...) — src/gpu/initMethods.jl:91-222 (src/cpu/initMethods.jl:89-222
+    under the CPU module's particle rules, whose addSquirmer! has no angularVelocity keyword)."""
+    if model._res.cfg.particle_rules == capi.LBM_RULES_CPU_MODULE and "angularVelocity" in kw:
+        raise TypeError('addSquirmer! got unsupported keyword argument "angularVelocity"')
     _add(model, cfgmod.resolve_squirmer(model._dims, **kw))
 
 
@@ -200,9 +223,26 @@ def addBead(model: LBMmodel, **kw) -> None:
 def LBMpropagate(model: LBMmodel, simulationTime=DEFAULT, ticks=DEFAULT, verbose=False, ticksSaved=DEFAULT) -> None:
     """LBMpropagate!(model; simulationTime, ticks, verbose, ticksSaved) — src/gpu/fluids.jl:228-264."""
     n = cfgmod.propagate_ticks(model.spaceTime.timeStep, simulationTime, ticks)
-    model.step(n)
+    if interactions.time_dependent(model):  # a field B(t) of dipoles: evaluated at each tick's time
+        if "saveData" in model.schemes:
+            raise NotImplementedError("saveData with a time-dependent magnetic field")
+        for _ in range(n):
+            interactions.push(model, model.time + model.spaceTime.timeStep)
+            model.step(1)
+    elif "saveData" in model.schemes:
+        output.propagate(model, n, None if ticksSaved is DEFAULT else ticksSaved)
+    else:
+        model.step(n)
     if verbose:
         print(f"\r t = {round(model.time, 2)}")
+
+
+def viscousStressTensor(model: LBMmodel):
+    """viscousStressTensor(model) — src/cpu/fluids.jl:507-520: a d x d matrix
+    whose entry (alpha, beta) is the field sigma_alpha_beta (N...)."""
+    s = model.viscous_stress_tensor()
+    d = model._dims
+    return [[s[..., a, b] for b in range(d)] for a in range(d)]
 
 
 def hydroVariablesUpdate(model: LBMmodel, useEquilibriumScheme=False) -> None:

@@ -26,6 +26,8 @@
  *   getNodeVelocity           src/gpu/aux.jl:229-263, kernels src/gpu/kernels.jl:376-415
  *   moveParticles!            src/gpu/particles.jl:7-92
  *   cross (2D/3D)             src/gpu/aux.jl:139-157
+ *   viscousStressTensor       src/cpu/fluids.jl:507-520 (nonEquilibriumDistribution :65-67)
+ *   molecularDynamicsTick!    src/gpu/particles.jl:100-197 (applyInteraction!, per interaction kind)
  * CPU-module particle rules (lbm_config.particle_rules == LBM_RULES_CPU_MODULE):
  *   moveParticles! / eulerStep!  src/cpu/particles.jl:7-18, :48-100
  *   bulkVelocity              src/cpu/particles.jl:21-46, cross src/cpu/aux.jl:19-28
@@ -118,6 +120,14 @@ template <int K> Dual<K> cos(const Dual<K>& a) {
     return r;
 }
 inline double val(double x) { return x; }
+inline double acos_(double x) { return std::acos(x); }
+template <int K> Dual<K> acos_(const Dual<K>& a) {
+    Dual<K> r;
+    r.v = std::acos(a.v);
+    const double g = -1.0 / std::sqrt(1.0 - a.v * a.v);
+    for (int k = 0; k < K; ++k) r.d[k] = g * a.d[k];
+    return r;
+}
 template <int K> double val(const Dual<K>& x) { return x.v; }
 using std::cos;
 using std::fabs;
@@ -135,6 +145,7 @@ struct Particle {
     int id = 0;
     int kind = LBM_SQUIRMER;
     bool couple_f = false, couple_t = false;
+    bool record_f = false;  // accumulate the momentum-exchange force without applying it (force observable)
     double radius = 0;
     Real B1 = 0, B2 = 0;
     double inv_mass = 0, inv_inertia = 0;
@@ -170,6 +181,7 @@ struct Model {
     int64_t tick = 0;
     double time = 0;
     int rules = LBM_RULES_GPU_MODULE;
+    std::vector<lbm_interaction> inter;  // particleInteractions, pairs flattened in order
     // bit id of wmark[c]: c is fluid and c - c_id a wall node (the walls'
     // streamingInvasionRegions of the opposite direction); mark[c] adds the
     // particles' regions for the current tick
@@ -672,6 +684,108 @@ void build_marks(Model<Real>& m) {
             }
 }
 
+// LinearAlgebra.norm of a d-vector: 0 for the zero vector, else sqrt of the
+// squares summed in component order
+template <class V>
+V vnorm(const V* v, int d) {
+    double mx = 0.0;
+    for (int k = 0; k < d; ++k) mx = std::max(mx, std::fabs(val(v[k])));
+    if (mx == 0.0) return V(0.0);
+    V s = v[0] * v[0];
+    for (int k = 1; k < d; ++k) s += v[k] * v[k];
+    return sqrt(s);
+}
+
+// applyInteraction! (src/gpu/particles.jl:111-197) of one item into the
+// particles' force inputs, from their current positions
+template <class Real>
+void apply_interaction(Model<Real>& m, const lbm_interaction& it) {
+    const int d = m.dims;
+    auto& P1 = m.parts[it.id1 - 1];
+    auto& P2 = m.parts[it.id2 - 1];
+    if (it.kind == LBM_INTERACTION_POLAR) {
+        auto& P3 = m.parts[it.id3 - 1];
+        Real d12[3] = {0, 0, 0}, d32[3] = {0, 0, 0}, u12[3] = {0, 0, 0}, u32[3] = {0, 0, 0};
+        for (int k = 0; k < d; ++k) {
+            d12[k] = P1.R[k] - P2.R[k];
+            d32[k] = P3.R[k] - P2.R[k];
+        }
+        const Real n12 = vnorm(d12, d), n32 = vnorm(d32, d);
+        for (int k = 0; k < d; ++k) {
+            u12[k] = d12[k] / n12;
+            u32[k] = d32[k] / n32;
+        }
+        Real x = u12[0] * u32[0];
+        for (int k = 1; k < d; ++k) x += u12[k] * u32[k];
+        if (std::fabs(val(x)) > 1.0) x = val(x) > 0 ? Real(1.0) : Real(-1.0);
+        const Real ang = acos_(x);
+        Real td[3] = {0, 0, 0};
+        cross_ref(d, u32, u12, td);
+        const Real an = d == 2 ? fabs(td[0]) : vnorm(td, 3);
+        if (val(an) > 0)
+            for (int k = 0; k < 3; ++k) td[k] = td[k] / an;
+        const Real s = it.p[1] * (ang - it.p[0]);
+        Real f321[3] = {0, 0, 0}, f123[3] = {0, 0, 0};
+        if (d == 2) {  // cross(omega::Real, V) = cross([0; 0; omega], [V; 0])[1:2]
+            const Real w = s * td[0];
+            f321[0] = 0.0 * 0.0 - w * u12[1];
+            f321[1] = -0.0 * 0.0 + w * u12[0];
+            f123[0] = 0.0 * 0.0 - w * u32[1];
+            f123[1] = -0.0 * 0.0 + w * u32[0];
+        } else {
+            const Real tq[3] = {s * td[0], s * td[1], s * td[2]};
+            cross_ref(3, tq, u12, f321);
+            cross_ref(3, tq, u32, f123);
+        }
+        Real a[3], b[3];
+        for (int k = 0; k < d; ++k) {
+            a[k] = -f321[k] / n12;
+            b[k] = f123[k] / n32;
+        }
+        for (int k = 0; k < d; ++k) P1.F[k] += a[k];
+        for (int k = 0; k < d; ++k) P3.F[k] += b[k];
+        for (int k = 0; k < d; ++k) P2.F[k] -= a[k] + b[k];
+        return;
+    }
+    Real dv[3] = {0, 0, 0}, u[3] = {0, 0, 0};
+    for (int k = 0; k < d; ++k) dv[k] = P2.R[k] - P1.R[k];  // disp21
+    const Real dist = vnorm(dv, d);
+    for (int k = 0; k < d; ++k) u[k] = dv[k] / dist;
+    Real f[3] = {0, 0, 0};
+    if (it.kind == LBM_INTERACTION_LINEAR) {
+        for (int k = 0; k < d; ++k) f[k] = it.p[1] * (dist - it.p[0]) * u[k];
+    } else if (it.kind == LBM_INTERACTION_BISTABLE) {
+        const Real x = dist - it.p[0];
+        for (int k = 0; k < d; ++k) f[k] = (it.p[1] * (x * x * x) - it.p[2] * x) * u[k];
+    } else if (it.kind == LBM_INTERACTION_LENNARD_JONES) {
+        if (!(val(dist) < it.p[2])) return;
+        const Real sd = it.p[1] / dist;
+        const Real s2 = sd * sd, s6 = s2 * s2 * s2;
+        for (int k = 0; k < d; ++k) f[k] = -4.0 * it.p[0] / dist * (12.0 * (s6 * s6) - 6.0 * s6) * u[k];
+    } else {  // dipoles, unless the field is zero (!(norm(B) ~ 0) with atol 0)
+        const double B[3] = {it.p[1], it.p[2], it.p[3]};
+        if (vnorm(B, d) == 0.0) return;
+        Real cb[3] = {0, 0, 0}, ccb[3] = {0, 0, 0};
+        cross_ref(d, u, B, cb);
+        Real sq;
+        if (d == 2) {
+            ccb[0] = 0.0 * 0.0 - cb[0] * B[1];
+            ccb[1] = -0.0 * 0.0 + cb[0] * B[0];
+            sq = cb[0] * cb[0];
+        } else {
+            cross_ref(3, cb, B, ccb);
+            sq = cb[0] * cb[0] + cb[1] * cb[1] + cb[2] * cb[2];
+        }
+        double bb = B[0] * B[0];
+        for (int k = 1; k < d; ++k) bb += B[k] * B[k];
+        const Real d2 = dist * dist;
+        const Real pre = -it.p[0] / (d2 * d2);
+        for (int k = 0; k < d; ++k) f[k] = pre * (2.0 * ccb[k] - 2.0 * bb * u[k] + 5.0 * u[k] * sq);
+    }
+    for (int k = 0; k < d; ++k) P1.F[k] += f[k];
+    for (int k = 0; k < d; ++k) P2.F[k] -= f[k];
+}
+
 template <class Real>
 void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
     const int64_t N = m.N;
@@ -733,8 +847,8 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
                     }
                     s[x] += (2 * wi * m.invC2) * m.rho[x] * dot_c(up, ci, d);
                 }
-                if (p.couple_f || p.couple_t) {
-                    if (p.couple_f) {
+                if (p.couple_f || p.couple_t || p.record_f) {
+                    if (p.couple_f || p.record_f) {
                         Real S = 0.0;
                         for (int64_t x : nodes) S += fsb[x] + s[x];
                         if (cpu) {  // momentumInput[id] -= dx^d sum(sumTerm) c (dx/dt)
@@ -771,8 +885,10 @@ void tick(Model<Real>& m, std::vector<Real>& fs, std::vector<Real>& fn) {
     m.time += m.dt;
     m.tick += 1;
     hydro(m);
-    if (m.ladd)
+    if (m.ladd) {  // molecularDynamicsTick! (src/gpu/particles.jl:100-107)
+        for (const auto& it : m.inter) apply_interaction(m, it);
         for (auto& p : m.parts) move(m, p, false);
+    }
 }
 
 template <class Real>
@@ -1068,6 +1184,32 @@ int orc_set_particle(void* hp, int32_t id, const lbm_particle_state* st) {
     return LBM_OK;
 }
 
+// particleInteractions: the items of lbm_set_interactions (pairs flattened,
+// 1-based ids), applied every tick before the particles move
+int orc_set_interactions(void* hp, const lbm_interaction* list, int32_t n) {
+    if (!hp || n < 0 || (n > 0 && !list)) return fail(LBM_ERR_INVALID, "bad interaction list");
+    Model<double>& m = static_cast<Handle*>(hp)->m;
+    const int np = (int)m.parts.size();
+    for (int t = 0; t < n; ++t)
+        if (list[t].id1 < 1 || list[t].id1 > np || list[t].id2 < 1 || list[t].id2 > np ||
+            (list[t].kind == LBM_INTERACTION_POLAR && (list[t].id3 < 1 || list[t].id3 > np)))
+            return fail(LBM_ERR_INVALID, "interaction names no valid particles");
+    m.inter.assign(list, list + n);
+    return LBM_OK;
+}
+
+// Accumulate particle `id`'s momentum-exchange force even when coupleForces
+// is off (`on` != 0), reporting it as last_force without applying it: the
+// drag of a held particle.  The reference accumulates no force for such a
+// particle; this switch exists for the force observable of the gradients.
+int orc_record_force(void* hp, int32_t id, int32_t on) {
+    if (!hp) return fail(LBM_ERR_INVALID, "null handle");
+    Model<double>& m = static_cast<Handle*>(hp)->m;
+    if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
+    m.parts[id - 1].record_f = on != 0;
+    return LBM_OK;
+}
+
 int orc_get_mask(void* hp, int32_t id, uint8_t* mask) {
     if (!hp || !mask) return fail(LBM_ERR_INVALID, "null argument");
     Model<double>& m = static_cast<Handle*>(hp)->m;
@@ -1110,6 +1252,43 @@ int orc_get_info(void* hp, lbm_info* info) {
     info->time = m.time;
     info->num_particles = (int32_t)m.parts.size();
     info->bytes_per_population = 8;
+    return LBM_OK;
+}
+
+// viscousStressTensor (src/cpu/fluids.jl:507-520): sigma_ab = -(1 - dt/(2 tau))
+// sum_i c_ia c_ib (f_i - f_eq_i), f_eq of equilibriumDistribution
+// (src/gpu/fluids.jl:39-52) at the model's rho and u, the sum over i a left
+// fold; out (N..., d, d) column-major
+int orc_get_stress(void* hp, double* out) {
+    if (!hp || !out) return fail(LBM_ERR_INVALID, "null argument");
+    const Model<double>& m = static_cast<Handle*>(hp)->m;
+    const int64_t N = m.N;
+    const int d = m.dims, Q = m.vs.q;
+    const double coeff = 1 - 0.5 * m.dt / m.tau;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < N; ++c) {
+        double neq[27];
+        double uu = 0.0;
+        for (int k = 0; k < d; ++k) uu += m.u[(int64_t)k * N + c] * m.u[(int64_t)k * N + c];
+        for (int i = 0; i < Q; ++i) {
+            double uc = 0.0;
+            for (int k = 0; k < d; ++k) uc += m.u[(int64_t)k * N + c] * (double)m.vs.c[i][k];
+            const double first = uc * m.invC2 + (uc * uc) * (0.5 * m.invC4);
+            const double second = first - uu * (0.5 * m.invC2);
+            const double wi = m.vs.w[i];
+            const double feq = m.compressible ? wi * ((second + 1) * m.rho[c]) : wi * m.rho[c] + wi * (m.rho0[c] * second);
+            neq[i] = m.f[(int64_t)i * N + c] - feq;
+        }
+        for (int b = 0; b < d; ++b)
+            for (int a = 0; a < d; ++a) {
+                double sum = 0.0;
+                for (int i = 0; i < Q; ++i) {
+                    const double t = (double)(m.vs.c[i][a] * m.vs.c[i][b]) * neq[i];
+                    sum = i == 0 ? t : sum + t;
+                }
+                out[c + N * (a + (int64_t)d * b)] = -coeff * sum;
+            }
+    }
     return LBM_OK;
 }
 
@@ -1169,6 +1348,28 @@ int ord_particle(void* hp, int32_t id, double* values, double* derivs) {
             values[3 * g + k] = x.v;
             for (int q = 0; q < kDirs; ++q) derivs[(size_t)(3 * g + k) * kDirs + q] = x.d[q];
         }
+    return LBM_OK;
+}
+
+int ord_record_force(void* hp, int32_t id, int32_t on) {
+    if (!hp) return fail(LBM_ERR_INVALID, "null handle");
+    Model<D6>& m = static_cast<DualHandle*>(hp)->m;
+    if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
+    m.parts[id - 1].record_f = on != 0;
+    return LBM_OK;
+}
+
+// momentum-exchange force of the last tick of particle `id`: values [3],
+// derivatives [3][kDirs]
+int ord_particle_force(void* hp, int32_t id, double* values, double* derivs) {
+    if (!hp || !values || !derivs) return fail(LBM_ERR_INVALID, "null argument");
+    const Model<D6>& m = static_cast<DualHandle*>(hp)->m;
+    if (id < 1 || id > (int32_t)m.parts.size()) return fail(LBM_ERR_INVALID, "no such particle");
+    const Particle<D6>& p = m.parts[id - 1];
+    for (int k = 0; k < 3; ++k) {
+        values[k] = p.lastF[k].v;
+        for (int q = 0; q < kDirs; ++q) derivs[(size_t)k * kDirs + q] = p.lastF[k].d[q];
+    }
     return LBM_OK;
 }
 

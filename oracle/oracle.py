@@ -60,6 +60,11 @@ def load() -> C.CDLL:
     lib.orc_get_particles.argtypes = [vp, C.POINTER(capi.LbmParticleState), C.c_int32, C.POINTER(C.c_int32)]
     lib.orc_get_mask.argtypes = [vp, C.c_int32, C.POINTER(C.c_uint8)]
     lib.orc_set_particle.argtypes = [vp, C.c_int32, C.POINTER(capi.LbmParticleState)]
+    lib.orc_record_force.argtypes = [vp, C.c_int32, C.c_int32]
+    lib.orc_get_stress.argtypes = [vp, dp]
+    lib.orc_set_interactions.argtypes = [vp, C.POINTER(capi.LbmInteraction), C.c_int32]
+    lib.ord_record_force.argtypes = [vp, C.c_int32, C.c_int32]
+    lib.ord_particle_force.argtypes = [vp, C.c_int32, dp, dp]
     lib.orc_get_links.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.c_int64,
                                   C.POINTER(C.c_int64)]
     lib.orc_get_info.argtypes = [vp, C.POINTER(capi.LbmInfo)]
@@ -132,6 +137,12 @@ class OracleModel:
         _check(self.lib.orc_get_fields(self.h, rho.ctypes.data_as(capi._dp), u.ctypes.data_as(capi._dp)))
         return rho, u.reshape(self.dims, self.cells)
 
+    def stress(self):
+        """viscousStressTensor: (d, d, N) with entry [a, b] the field sigma_ab."""
+        s = np.zeros(self.cells * self.dims * self.dims, dtype=np.float64)
+        _check(self.lib.orc_get_stress(self.h, s.ctypes.data_as(capi._dp)))
+        return s.reshape(self.dims, self.dims, self.cells).transpose(1, 0, 2)
+
     def distributions(self):
         f = np.zeros(self.cells * self.q, dtype=np.float64)
         _check(self.lib.orc_get_distributions(self.h, f.ctypes.data_as(capi._dp)))
@@ -152,6 +163,16 @@ class OracleModel:
         """Move particle `pid` to another state (position, velocity, angular velocity,
         swimming direction of an LbmParticleState) and re-voxelise it there."""
         _check(self.lib.orc_set_particle(self.h, pid, C.byref(state)))
+
+    def set_interactions(self, items) -> None:
+        """particleInteractions as a list of LbmInteraction items (pairs flattened in order)."""
+        arr = (capi.LbmInteraction * max(1, len(items)))(*items)
+        _check(self.lib.orc_set_interactions(self.h, arr, len(items)))
+
+    def record_force(self, pid: int, on: bool = True) -> None:
+        """Accumulate particle pid's momentum-exchange force even when it is not
+        coupled (reported as last_force, never applied): the drag of a held particle."""
+        _check(self.lib.orc_record_force(self.h, pid, int(bool(on))))
 
     def mask(self, pid: int):
         m = np.zeros(self.cells, dtype=np.uint8)
@@ -236,6 +257,16 @@ class DualOracle:
         names = ("position", "velocity", "angular_velocity", "swimming_direction")
         return ({n: v[3 * i:3 * i + 3] for i, n in enumerate(names)},
                 {n: d[3 * i:3 * i + 3] for i, n in enumerate(names)})
+
+    def record_force(self, pid: int = 1, on: bool = True) -> None:
+        _check(self.lib.ord_record_force(self.h, pid, int(bool(on))))
+
+    def particle_force(self, pid: int = 1):
+        """(values (3,), derivatives (3, K)) of the last tick's momentum-exchange force."""
+        v = np.zeros(3)
+        d = np.zeros((3, self.K))
+        _check(self.lib.ord_particle_force(self.h, pid, v.ctypes.data_as(capi._dp), d.ctypes.data_as(capi._dp)))
+        return v, d
 
     def close(self):
         if self.h:

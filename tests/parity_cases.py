@@ -118,8 +118,8 @@ def particle_params(dims, p):
     return cfgmod.resolve_squirmer(dims, **p)
 
 
-def build_pair(case, storage="f64", oracle_mod=None, with_gpu=True):
-    res = cfgmod.resolve_model(**case["model"], storage=storage)
+def build_pair(case, storage="f64", oracle_mod=None, with_gpu=True, rules="gpu"):
+    res = cfgmod.resolve_model(**case["model"], storage=storage, particleRules=rules)
     gpu = lbmmodel.LBMmodel(res) if with_gpu else None
     orc = oracle_mod.OracleModel(res) if oracle_mod is not None else None
     for p in case["particles"]:

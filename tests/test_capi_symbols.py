@@ -95,8 +95,10 @@ def _c_fields(header, name):
         decl = decl.strip()
         if not decl:
             continue
-        m2 = re.search(r"(\w+)\s*(\[\s*\d+\s*\])?$", decl)
-        out.append(m2.group(1))
+        first, *rest = decl.split(",")  # "double B1, B2" declares two fields
+        for d in [first] + rest:
+            m2 = re.search(r"(\w+)\s*(\[\s*\d+\s*\])?$", d.strip())
+            out.append(m2.group(1))
     return out
 
 

@@ -209,3 +209,62 @@ def test_oracle_regression_fixture(oracle_mod):
         for p, gp in zip(orc.particles(), g["particles"]):
             np.testing.assert_allclose(p.position, gp["position"], rtol=1e-14, atol=0)
             np.testing.assert_allclose(p.last_force, gp["last_force"], rtol=1e-9, atol=1e-18)
+
+
+# ---- the CPU module's particle rules (lbm_config.particle_rules) -----------
+def _rules_pair(oracle_mod, model_kw, particles, steps):
+    out = []
+    for rules in ("gpu", "cpu"):
+        res = config.resolve_model(**model_kw, particleRules=rules)
+        m = oracle_mod.OracleModel(res)
+        for kind, kw in particles:
+            m.add_particle(config.resolve_bead(res.dims, **kw) if kind == "bead" else
+                           config.resolve_squirmer(res.dims, **kw))
+        m.step(steps)
+        out.append(m)
+    return out
+
+
+_MODEL_2D = dict(dims=2, latticeParameter=1.0, relaxationTimeRatio=0.8, collisionModel="trt",
+                 xlims=(-16.0, 15.0), forceDensity=[1e-5, 0.0])
+
+
+def test_rules_agree_exactly_where_the_modules_coincide(oracle_mod):
+    """A coupled 2D bead: the two modules' updates are the same operations
+    (v += m^-1 dt F with dt = dx = 1, the 2D cross products of both modules
+    agree), so fields and trajectory agree bit for bit."""
+    g, c = _rules_pair(oracle_mod, _MODEL_2D, [("bead", dict(radius=4.0, position=[0.3, -0.2], coupleForces=True,
+                                                             coupleTorques=True, massDensity=2.0))], 80)
+    rg, ug = g.fields()
+    rc, uc = c.fields()
+    np.testing.assert_array_equal(rg, rc)
+    np.testing.assert_array_equal(ug, uc)
+    pg, pc = g.particles()[0], c.particles()[0]
+    assert list(pg.position) == list(pc.position) and list(pg.velocity) == list(pc.velocity)
+    assert list(pg.angular_velocity) == list(pc.angular_velocity)
+
+
+def test_cpu_rules_never_rotate_the_swimming_direction(oracle_mod):
+    sq = dict(radius=4.0, position=[0.3, -0.2], swimmingSpeed=2e-3, beta=3.0, swimmingDirection=[0.6, 0.8],
+              coupleForces=True, coupleTorques=True, massDensity=2.0)
+    g, c = _rules_pair(oracle_mod, _MODEL_2D, [("squirmer", sq)], 120)
+    pg, pc = g.particles()[0], c.particles()[0]
+    assert pc.angular_velocity[0] != 0.0  # it spins ...
+    np.testing.assert_allclose(pc.swimming_direction[:2], [0.6, 0.8], rtol=0, atol=1e-15)  # ... but e stays
+    assert abs(pg.swimming_direction[0] - 0.6) > 1e-9  # the GPU module rotates e
+
+
+def test_cpu_rules_move_uncoupled_particles_with_their_velocity(oracle_mod):
+    """src/cpu/particles.jl:59: the Euler step runs whenever v != 0, coupled or not."""
+    bead = dict(radius=3.0, position=[0.25, 0.0], velocity=[1e-2, 0.0], coupleForces=False, coupleTorques=False)
+    g, c = _rules_pair(oracle_mod, _MODEL_2D, [("bead", bead)], 50)
+    assert list(g.particles()[0].position[:2]) == [0.25, 0.0]
+    np.testing.assert_allclose(c.particles()[0].position[:2], [0.25 + 50 * 1e-2, 0.0], rtol=0, atol=1e-13)
+    assert list(c.particles()[0].velocity[:2]) == [1e-2, 0.0]
+
+
+def test_rules_share_the_fluid_step(oracle_mod):
+    """Without particles the two rules are the same model."""
+    kw = dict(_MODEL_2D, walledDimensions=[2])
+    g, c = _rules_pair(oracle_mod, kw, [], 60)
+    np.testing.assert_array_equal(g.distributions(), c.distributions())

@@ -13,8 +13,10 @@ component):
     <= 1e-5, velocity <= 1e-4, positions <= 1e-7;
   * FP16 / BF16 storage (shifted by w_i rho0, scaled by 2^12, FP32 collision,
     dithered stochastic rounding, FP64 particles): the values of TOL below,
-    about three times the largest error measured on these cases; FP16 meets
-    the velocity target of 1e-3.
+    about three times the largest error measured on these cases (short runs
+    with weak flows, where the relative velocity error of FP16 is up to
+    ~7e-4; the FP16 target of 1e-3 is checked on the 128^3 workload in
+    test_configs_gpu.py).
 Torque errors are relative to max(|T|, |F| r) of the oracle: the net torque of
 a nearly symmetric particle is a small difference of terms of size |F| r (a
 centred bead's is pure rounding, ~1e-14).
@@ -33,8 +35,8 @@ pytestmark = pytest.mark.gpu
 
 TOL = {"f64": dict(field=1e-10, u=1e-10, pos=1e-10, vel=1e-10, force=1e-8, torque=1e-8),
        "f32": dict(field=1e-5, u=1e-4, pos=1e-7, vel=1e-7, force=5e-4, torque=5e-4),
-       "f16": dict(field=3e-6, u=1e-3, pos=6e-5, vel=5e-7, force=2e-2, torque=2e-2),
-       "bf16": dict(field=1.5e-5, u=2.5e-2, pos=1e-4, vel=1e-5, force=0.35, torque=0.35)}
+       "f16": dict(field=3e-6, u=2e-3, pos=5e-5, vel=2e-6, force=5e-2, torque=1e-1),
+       "bf16": dict(field=1e-4, u=5e-2, pos=3e-3, vel=1e-4, force=0.8, torque=0.8)}
 
 
 def _angular(s, d):
@@ -106,6 +108,22 @@ def test_parity_fields_and_trajectories(lib, oracle_mod, name, storage):
     compare_state(res, gpu, orc, tol, f"{name}/{storage}/t{steps}")
 
 
+@pytest.mark.parametrize("name", ["d2q9_bgk_squirmer", "d3q19_multi", "d3q19_trt_guo_squirmer", "d2q9_bgk_lid_bead"])
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_parity_under_cpu_module_rules(lib, oracle_mod, name, storage):
+    """The CPU module's particle update (src/cpu/particles.jl:7-106): Euler step
+    whenever v != 0, no rotation of the swimming direction, its bulkVelocity."""
+    case = CASES[name]
+    res, gpu, orc = build_pair(case, storage=storage, oracle_mod=oracle_mod, rules="cpu")
+    tol = TOL[storage]
+    steps = case["steps"]
+    gpu.step(steps // 3)
+    orc.step(steps // 3)
+    gpu.step(steps - steps // 3)
+    orc.step(steps - steps // 3)
+    compare_state(res, gpu, orc, tol, f"{name}/{storage}/cpu-rules/t{steps}")
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_masks_and_links_bit_exact(lib, oracle_mod, name):
     case = CASES[name]
@@ -153,3 +171,25 @@ def test_mass_conservation_periodic(lib):
     m0 = m.massDensity.sum()
     m.step(200)
     assert abs(m.massDensity.sum() - m0) / m0 < 1e-6
+
+
+@pytest.mark.parametrize("name", ["d2q9_trt_channel", "d3q19_trt_guo_squirmer", "d2q9_incompressible",
+                                  "d2q9_bgk_lid_bead"])
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_viscous_stress_tensor(lib, oracle_mod, name, storage):
+    """viscousStressTensor (src/cpu/fluids.jl:507-520) on the device against the oracle."""
+    case = CASES[name]
+    res, gpu, orc = build_pair(case, storage=storage, oracle_mod=oracle_mod)
+    gpu.step(case["steps"])
+    orc.step(case["steps"])
+    sg = gpu.viscous_stress_tensor()  # (N..., d, d)
+    so = orc.stress()                 # (d, d, N)
+    d = res.dims
+    scale = np.max(np.abs(so))
+    assert scale > 0
+    for a in range(d):
+        for b in range(d):
+            g = sg[..., a, b].ravel(order="F")
+            tol = 1e-9 if storage == "f64" else 2e-3
+            assert np.max(np.abs(g - so[a, b])) <= tol * scale, (a, b)
+    np.testing.assert_allclose(sg[..., 0, 1], sg[..., 1, 0], rtol=0, atol=1e-15 * scale + 1e-300)
