@@ -42,6 +42,17 @@ def unit_vector(seed, dims):
     return list(v / np.sqrt((v * v).sum()))
 
 
+# The body force accelerates the whole periodic box (u_x = 1e-6 t), so the
+# squirmer of the 128^3 workload is carried x ~ 5e-7 t^2 and reaches the x
+# boundary near tick 10,550.  There the reference's particle geometry is not
+# periodic: the torque arm and the slip velocity use the unwrapped X - R
+# (src/gpu/fluids.jl:206-208, src/gpu/particles.jl getNodeVelocity), so a link
+# across the boundary gets an arm of about one box length and the coupling
+# diverges in every storage format, FP64 included (near tick 11,000).  The
+# default timed run (200 warm-up + 10,000 ticks) ends before the crossing.
+VALID_TICKS_128 = 10_500
+
+
 def workload(side=128, storage="f32", device=-1):
     """The 128^3 D3Q19 TRT squirmer workload (coordinates centred on the origin)."""
     h = side // 2
@@ -62,6 +73,8 @@ def workload_name(side, storage=None):
 def bench_config(side, world):
     """The `config` object of the JSON line; both arms print the same one."""
     return {"workload": workload_name(side), "cells": side ** 3,
+            "ticks_valid": f"the squirmer crosses the periodic x boundary near tick {VALID_TICKS_128} (128^3), "
+                           "after which the reference's unwrapped torque arm makes the coupling diverge",
             "parallelism": "replicas" if world > 1 else "single",
             "l2": f"inputs larger than L2: D3Q19 populations 2 x {side ** 3 * 19 * 4 / 1e6:.0f} MB (FP32)"}
 
@@ -184,8 +197,10 @@ ORACLE_SEMANTICS = ("FP64 C++ restatement of the reference's tick (fluid step of
                     "Julia and cannot run here")
 
 
-def oracle_mlups(side, ticks, warm, threads=None):
-    """FP64 CPU oracle on a side^3 box of the workload: (MLUPS, seconds, threads)."""
+def oracle_mlups(side, ticks, warm, threads=None, budget_s=None):
+    """FP64 CPU oracle on a side^3 box of the workload: (MLUPS, seconds, threads,
+    ticks timed).  With budget_s, at most the ticks that fit the budget are
+    timed (measured from the first warm-up tick), at least one."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle  # CPU baseline leg only
     from lbmengine import config
@@ -196,16 +211,20 @@ def oracle_mlups(side, ticks, warm, threads=None):
     res = config.resolve_model(**mkw)
     m = oracle.OracleModel(res)
     m.add_particle(config.resolve_squirmer(3, **skw))
-    m.step(warm)
+    t0 = time.perf_counter()
+    m.step(max(1, warm))
+    per_tick = (time.perf_counter() - t0) / max(1, warm)
+    if budget_s is not None:
+        ticks = max(1, min(ticks, int(budget_s / max(per_tick, 1e-9))))
     t0 = time.perf_counter()
     m.step(ticks)
     dt = time.perf_counter() - t0
-    return side ** 3 * ticks / dt / 1e6, dt, oracle.max_threads()
+    return side ** 3 * ticks / dt / 1e6, dt, oracle.max_threads(), ticks
 
 
 def oracle_side_for(ticks_total, budget_s):
     """Largest box (multiple of 8, 16..128) whose ticks fit the time budget."""
-    rate, _, _ = oracle_mlups(24, 2, 1)
+    rate, _, _, _ = oracle_mlups(24, 2, 1)
     cells = rate * 1e6 * budget_s / max(1, ticks_total)
     side = int(cells ** (1 / 3)) // 8 * 8
     return max(16, min(128, side))
@@ -216,15 +235,17 @@ def run_reference(args):
     if rank != 0:
         return 0
     side = args.side
-    mlups, dt, threads = oracle_mlups(side, args.steps, args.warmup)
+    # each timed tick is the full workload; at most ~60 s of CPU ticks are timed
+    warm = max(1, min(args.warmup, 3))
+    mlups, dt, threads, timed = oracle_mlups(side, args.steps, warm, budget_s=60.0)
     line = {
         "metric": METRIC, "impl": "reference", "value": round(mlups, 4), "unit": "MLUPS", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, args.steps),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": bench_config(side, world),
         "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": threads, "kind": "port",
-                         "sample": f"the full {side}^3 workload, {args.steps} ticks after {args.warmup} warm-up "
-                                   f"ticks on this host's cores; {ORACLE_SEMANTICS}"},
+                         "sample": f"the full {side}^3 workload, {timed} of the {args.steps} ticks (at most ~60 s) "
+                                   f"after {warm} warm-up ticks on this host's cores; {ORACLE_SEMANTICS}"},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -250,6 +271,9 @@ def run_ours(args):
     q = 19
     lib = m._lib
 
+    if side == 128 and max(3, args.warmup) + args.steps > VALID_TICKS_128:
+        print(f"bench: {max(3, args.warmup) + args.steps} ticks run past the periodic-boundary crossing near tick "
+              f"{VALID_TICKS_128}, where the reference's coupling diverges; expect LBM_ERR_NUMERIC", file=sys.stderr)
     m.step(max(3, args.warmup))
     barrier(dist)
     lib.lbm_set_profiling(m.handle, 1)
@@ -277,6 +301,7 @@ def run_ours(args):
     traffic = bulk_traffic(storage, prof.bulk_cells)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
+                "frac_of_nominal_8000": round(achieved / 8000.0, 4) if achieved else None,
                 "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "traffic_source": "replayed from an earlier ncu capture (profiles/bulk_traffic.txt), not this run",
@@ -319,7 +344,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ticks = args.cpu_ticks
-        mlups, dt, threads = oracle_mlups(side, ticks, 1)
+        mlups, dt, threads, _ = oracle_mlups(side, ticks, 1)
         cpu = {"value": round(mlups, 4), "unit": "MLUPS", "cores": threads, "kind": "port",
                "sample": f"{ticks} ticks (after 1 warm-up tick) of the full {side}^3 workload ({dt:.1f} s); "
                          f"{ORACLE_SEMANTICS}"}
@@ -573,12 +598,33 @@ def form_gradients(device, ticks=3000, window=(1000, 3000), dual_side=32, dual_t
         m = build_swimmer(mkw, skw, th)
         e0 = np.array(skw["swimmingDirection"])
         J = 0.0
+        track = []
         for t in range(1, ticks + 1):
             m.step(1)
+            st = m.particle_states()[0]
+            track.append(np.array(st.position[:3]))
             if window[0] <= t <= window[1]:
-                J += float(np.dot(m.particle_states()[0].velocity[:3], e0)) / (window[1] - window[0] + 1)
+                J += float(np.dot(st.velocity[:3], e0)) / (window[1] - window[0] + 1)
         m.close()
-        return J
+        return J, track
+
+    axis = np.arange(96, dtype=np.float64) - 48.0  # node coordinates of the 96^3 box
+
+    def flips(tp, tm, r=8.0):
+        """Nodes inside one run's sphere and outside the other's (the getSphere test
+        (x-R1)^2+(y-R2)^2+(z-R3)^2 < r^2 in FP64), summed over the ticks."""
+        total, ticks_with = 0, 0
+        for a, b in zip(tp, tm):
+            lo = np.floor(np.minimum(a, b) - r - 1).astype(int) + 48
+            hi = np.ceil(np.maximum(a, b) + r + 1).astype(int) + 48
+            x, y, z = (axis[max(0, lo[k]):min(96, hi[k] + 1)] for k in range(3))
+            X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+            ina = ((X - a[0]) * (X - a[0]) + (Y - a[1]) * (Y - a[1])) + (Z - a[2]) * (Z - a[2]) < r * r
+            inb = ((X - b[0]) * (X - b[0]) + (Y - b[1]) * (Y - b[1])) + (Z - b[2]) * (Z - b[2]) < r * r
+            n = int(np.count_nonzero(ina != inb))
+            total += n
+            ticks_with += n > 0
+        return {"node_flips": total, "ticks_with_flips": ticks_with}
 
     fd = {}
     for rel in (1e-4, 1e-6, 1e-8):
@@ -588,10 +634,44 @@ def form_gradients(device, ticks=3000, window=(1000, 3000), dual_side=32, dual_t
             tp, tm = theta.copy(), theta.copy()
             tp[k] += h
             tm[k] -= h
-            d = (observable(tp) - observable(tm)) / (2 * h)
+            (Jp, trp), (Jm, trm) = observable(tp), observable(tm)
+            d = (Jp - Jm) / (2 * h)
             fd[str(rel)][nm] = {"fd": d, "rel_err_f64_adjoint": abs(out["f64"]["grad"][nm] - d) / abs(d),
-                                "rel_err_f32_adjoint": abs(out["f32"]["grad"][nm] - d) / abs(d)}
+                                "rel_err_f32_adjoint": abs(out["f32"]["grad"][nm] - d) / abs(d),
+                                **flips(trp, trm)}
     out["central_differences"] = fd
+    # the drag of the same squirmer held in place: no node ever changes sides,
+    # so central differences at the configured step h = 1e-4 hold
+    from lbmengine.adjoint import drag_gradient
+    skw_held = dict(skw, coupleForces=False, coupleTorques=False)
+    m = build_swimmer(mkw, skw_held)
+    gd = drag_gradient(m, ticks, window, snapshots=32)
+    m.close()
+
+    def drag(th):
+        m = build_swimmer(mkw, skw_held, th)
+        m.record_force(1)
+        e0 = np.array(skw["swimmingDirection"])
+        J = 0.0
+        for t in range(1, ticks + 1):
+            m.step(1)
+            if window[0] <= t <= window[1]:
+                J += float(np.dot(m.particle_states()[0].last_force[:3], e0)) / (window[1] - window[0] + 1)
+        m.close()
+        return J
+
+    dfd = {}
+    for k, nm in enumerate(("B1", "B2", "tau", "Fx")):
+        h = 1e-4 * abs(theta[k])
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        d = (drag(tp) - drag(tm)) / (2 * h)
+        dfd[nm] = {"fd": d, "adjoint": gd.grad[nm], "rel_err": abs(gd.grad[nm] - d) / abs(d)}
+    out["drag"] = {"observable": "momentum-exchange force on the held squirmer along its orientation, averaged "
+                                 f"over ticks {window[0]}..{window[1]} (FP64 storage)",
+                   "value": gd.value, "ms": round(gd.ms, 1), "central_differences_h1e-4": dfd,
+                   "fd_rel_err_max": max(v["rel_err"] for v in dfd.values())}
     # forward-mode dual numbers through the CPU oracle on the same setup at dual_side^3
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle  # the checker
@@ -742,8 +822,13 @@ def forms_summary(forms):
         cd = f.get("central_differences", {})
         out["gradients_c5"] = {"s": round(f["f32"]["ms"] / 1e3, 1),
                                "dual_rel_err_max": _r(max(f["dual_check"]["rel_err"].values())),
-                               "fd_rel_err_max": {h: _r(max(v["rel_err_f64_adjoint"] for v in cd[h].values()))
-                                                  for h in cd}}
+                               # per step h and parameter: [FD vs adjoint rel. error, nodes that
+                               # changed sides between the +h and -h runs]
+                               "fd_err_and_flips": {h: {k: [_r(v["rel_err_f64_adjoint"], 2), v.get("node_flips")]
+                                                        for k, v in cd[h].items()} for h in cd},
+                               "fd_rel_err_max_flip_free": _r(max((v["rel_err_f64_adjoint"] for h in cd
+                                                                   for v in cd[h].values()
+                                                                   if v.get("node_flips") == 0), default=None))}
         if "drag" in f:
             out["gradients_c5"]["drag_fd_rel_err_max"] = f["drag"].get("fd_rel_err_max")
     f = forms.get("parity", {})
@@ -785,7 +870,7 @@ def run_forms(args, device):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16", "f64"], default="f32")

@@ -6,8 +6,8 @@
  * the exported Julia API (src/LBMengine.jl:27-41) and the fields of
  * `LBMmodel` / `LBMparticle` (src/gpu/structs.jl:52-95).  Each entry point
  * below names the reference function whose effect it reproduces; a Julia
- * shim binds them with `ccall`, a Python mirror binds
- * them with ctypes (lbmengine.jl_b200/lbmengine/_capi.py).
+ * shim binds them with `ccall` (lbmengine.jl_b200/julia/LBMengineB200.jl), a
+ * Python mirror binds them with ctypes (lbmengine.jl_b200/lbmengine/_capi.py).
  *
  * Conventions
  *   - Every function returns an int status: 0 = LBM_OK, < 0 = error.  The
@@ -269,6 +269,13 @@ int lbm_record_trajectories(lbm_handle* h, int64_t capacity);
 int lbm_read_trajectories(lbm_handle* h, double* out, int64_t capacity, int64_t* ticks);
 int lbm_write_fluid_csv(lbm_handle* h, const char* path);
 int lbm_output_flush(lbm_handle* h);
+
+/* Global sums over the lattice in FP64, on the device in a fixed order:
+ * mass = sum of rho, momentum = sum of rho u (the momentum density of
+ * hydroVariablesUpdate!, with the Guo half force; wall nodes contribute
+ * zero), in lattice units (multiply by dx^d for physical units).  No
+ * counterpart in the reference; for conservation checks. */
+int lbm_get_totals(lbm_handle* h, double* mass, double* momentum);
 
 /* model.distributions (N..., Q), FP64. */
 int lbm_get_distributions(lbm_handle* h, double* f);

@@ -55,6 +55,9 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     """Compile and link the library unless it is newer than every source."""
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= _deps_mtime():
         return OUT
+    # the sources as of now are what gets compiled; the library is stamped with
+    # this time, so a source edited while the build runs makes it stale
+    stamp = _deps_mtime()
     os.makedirs(BUILD, exist_ok=True)
     jobs = jobs or min(len(UNITS), os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -64,6 +67,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.utime(tmp, (stamp, stamp))
     os.replace(tmp, OUT)
     return OUT
 

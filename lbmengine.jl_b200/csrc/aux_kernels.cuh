@@ -146,6 +146,61 @@ __global__ void k_stress(const CodecArgs a) {
         for (int q = 0; q < D; ++q) a.stress[(p + D * q) * a.N + c] = -a.stress_coeff * s[p][q];
 }
 
+// Global FP64 sums of the density and the momentum density (rho, rho u with
+// the Guo half force, as hydroVariablesUpdate! forms them; wall nodes hold
+// zero), in a fixed order: every CTA sums its kTotBlock cells by a tree into
+// part[cta][4]; k_totals_final sums the CTA parts in CTA order.
+constexpr int kTotBlock = 256;
+
+template <class L, int ST>
+__global__ void __launch_bounds__(kTotBlock) k_totals(const CodecArgs a, double* part) {
+    using SS = Store<ST>;
+    using T = typename SS::T;
+    __shared__ double s[4][kTotBlock];
+    const long long c = blockIdx.x * (long long)kTotBlock + threadIdx.x;
+    double v[4] = {0, 0, 0, 0};
+    if (c < a.N && !(a.wall && a.wall[c])) {
+        const T* pop = static_cast<const T*>(a.pop);
+        double drho = 0, j[3] = {0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < L::Q; ++i) {
+            const double wg = L::w(i) * (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale);
+            drho += wg;
+            j[0] += L::cx(i) * wg;
+            j[1] += L::cy(i) * wg;
+            j[2] += L::cz(i) * wg;
+        }
+        v[0] = a.rho0 + drho;
+        for (int k = 0; k < L::D; ++k) {
+            const double F = a.force_mode == 1 ? a.F[k] : (a.force_mode == 2 ? a.ffield[k * a.N + c] : 0.0);
+            v[1 + k] = j[k] + a.half_dt * F;
+        }
+    }
+    for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int w = kTotBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 4; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+static __global__ void __launch_bounds__(kTotBlock) k_totals_final(const double* part, long long nblocks, double* out) {
+    __shared__ double s[4][kTotBlock];
+    double v[4] = {0, 0, 0, 0};
+    for (long long b = threadIdx.x; b < nblocks; b += kTotBlock)
+        for (int k = 0; k < 4; ++k) v[k] += part[b * 4 + k];
+    for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int w = kTotBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 4; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
 struct InitArgs {
     void* pop;
     long long N;
@@ -222,22 +277,6 @@ __global__ void k_mask(const MaskArgs a) {
     const int y = (int)((q / a.n[0]) % a.n[1]);
     const int z = (int)(q / ((long long)a.n[0] * a.n[1]));
     a.mask[q] = solid_at(*a.part, a.ivl, x, y, z) ? 1 : 0;
-}
-
-// device-side scan for non-finite or non-positive densities (fault detection)
-template <class L, int ST>
-__global__ void k_check(const CodecArgs a, int* bad) {
-    using SS = Store<ST>;
-    using T = typename SS::T;
-    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= a.N) return;
-    if (a.wall && a.wall[c]) return;
-    const T* pop = static_cast<const T*>(a.pop);
-    double drho = 0;
-#pragma unroll
-    for (int i = 0; i < L::Q; ++i) drho += L::w(i) * (double)SS::dec(pop[i * a.N + c], (typename SS::R)a.inv_scale);
-    const double rho = a.rho0 + drho;
-    if (!(rho > 0.0) || !isfinite(rho)) atomicOr(bad, 1);
 }
 
 }  // namespace lbm

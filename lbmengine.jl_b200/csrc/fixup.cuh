@@ -61,10 +61,10 @@ __device__ __forceinline__ void ladd_link(const StepArgs& a, const ParticleDev& 
 }
 
 // One CTA per kFixBlock link entries, NT threads (NT >= kFixBlock).
-//   round 1: the particle record, the entry (cell, mask) of threads < kFixBlock
+//   first loads: the particle record, the entry (cell, mask) of threads < kFixBlock
 //            ((link_off, link_cap) of the first particles come with the
 //            kernel parameters, so the entry load does not wait for the record)
-//   round 2: each entry's populations and the coordinates of its node and of
+//   second loads: each entry's populations and the coordinates of its node and of
 //            the node's +-1 neighbours per axis (every link target x + c_i is
 //            among them); the node is collided once into shared memory and
 //            the links of all entries are listed (entry, j)
@@ -153,7 +153,7 @@ __device__ __forceinline__ bool fixup_body(const StepArgs& a, const long long b)
     }
     if (tid == 0) s_alone = 1;
     __syncthreads();
-    // round 2 loads first: populations and coordinates of each entry's node
+    // the second loads first: populations and coordinates of each entry's node
     const unsigned mask = valid ? (unsigned)ent.y : 0u;
     NodeState<L, ST, TRT> st;
     double cc[3][3];

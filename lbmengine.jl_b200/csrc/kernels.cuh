@@ -519,9 +519,12 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
 // ---------------------------------------------------------------------------
 template <int ST> struct Vec4;
 template <> struct Vec4<ST_F32> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
-        const float4 q = __ldcs(reinterpret_cast<const float4*>(static_cast<const float*>(base) + cell0));
+    using raw = float4;  // the four values as stored
+    static __device__ __forceinline__ void unpack(const raw& q, float* v) {
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    }
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
+        unpack(__ldcs(reinterpret_cast<const float4*>(static_cast<const float*>(base) + cell0)), v);
     }
     // values of direction `dir` for cells cell0 .. cell0+3 (cell0 a multiple of 4)
     static __device__ __forceinline__ void store(void* base, int cell0, int, float a0, float a1, float a2, float a3,
@@ -532,11 +535,14 @@ template <> struct Vec4<ST_F32> {
     }
 };
 template <> struct Vec4<ST_F16> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
-        const uint2 q = __ldcs(reinterpret_cast<const uint2*>(static_cast<const __half*>(base) + cell0));
+    using raw = uint2;
+    static __device__ __forceinline__ void unpack(const raw& q, float* v) {
         const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
         const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
+    }
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
+        unpack(__ldcs(reinterpret_cast<const uint2*>(static_cast<const __half*>(base) + cell0)), v);
     }
     // rounding to nearest (dither null) or stochastic with the group's dither
     // words (storage.cuh): cell k of direction dir adds word (k + dir) mod 4
@@ -556,11 +562,14 @@ template <> struct Vec4<ST_F16> {
     }
 };
 template <> struct Vec4<ST_BF16> {
-    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
-        const uint2 q = __ldcs(reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + cell0));
+    using raw = uint2;
+    static __device__ __forceinline__ void unpack(const raw& q, float* v) {
         const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.x));
         const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.y));
         v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
+    }
+    static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
+        unpack(__ldcs(reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + cell0)), v);
     }
     static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
                                                  float a3, const unsigned* dither) {
@@ -591,6 +600,31 @@ constexpr int x_slot(int i) {  // exchange slot of direction i (cx != 0)
     return n;
 }
 
+
+// The pushes of one thread's four x-nodes (x0 .. x0+3 of row (y, z)) after
+// their collision: direction i goes to x + c_i with aligned vector stores.
+// from_left(i) / from_right(i) give the value of the +x / -x moving direction
+// i that the neighbouring segment pushes into this one (read next to the
+// store that needs it, so that the exchanged values are not all live at once).
+template <class L, int ST, class FromLeft, class FromRight>
+__device__ __forceinline__ void bulk_v4_push(const StepArgs& a, const float (&g)[4][L::Q], FromLeft from_left,
+                                             FromRight from_right, int x0, int y, int z, const unsigned* dither) {
+    constexpr int Q = L::Q;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+    const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int t0 = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
+        if (L::cx(i) == 0) {
+            Vec4<ST>::store(a.dstq[i], t0, i, g[0][i], g[1][i], g[2][i], g[3][i], dither);
+        } else if (L::cx(i) == 1) {
+            Vec4<ST>::store(a.dstq[i], t0, i, from_left(i), g[0][i], g[1][i], g[2][i], dither);
+        } else {
+            Vec4<ST>::store(a.dstq[i], t0, i, g[1][i], g[2][i], g[3][i], from_right(i), dither);
+        }
+    }
+}
 
 // One tile of the vector bulk pass: `a.vrows` full x-rows of one z-slice, four
 // consecutive x-nodes per thread with 128-bit (FP32) or 64-bit (FP16/BF16)
@@ -647,19 +681,9 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
     if (!valid) return;
     const int left = row * RT + (j == 0 ? RT - 1 : j - 1);
     const int right = row * RT + (j == RT - 1 ? 0 : j + 1);
-    const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
-    const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        const int t0 = x0 + nx * (ys[L::cy(i) + 1] + ny * zs[L::cz(i) + 1]);
-        if (L::cx(i) == 0) {
-            Vec4<ST>::store(a.dstq[i], t0, i, g[0][i], g[1][i], g[2][i], g[3][i], dither);
-        } else if (L::cx(i) == 1) {
-            Vec4<ST>::store(a.dstq[i], t0, i, s_ex[x_slot<L>(i)][left], g[0][i], g[1][i], g[2][i], dither);
-        } else {
-            Vec4<ST>::store(a.dstq[i], t0, i, g[1][i], g[2][i], g[3][i], s_ex[x_slot<L>(i)][right], dither);
-        }
-    }
+    bulk_v4_push<L, ST>(
+        a, g, [&](int i) { return s_ex[x_slot<L>(i)][left]; }, [&](int i) { return s_ex[x_slot<L>(i)][right]; }, x0,
+        y, z, dither);
 }
 
 // Resident threads per SM the vector bulk kernels are compiled for: a D2Q9

@@ -751,6 +751,15 @@ int check_device_error(lbm_handle* h) {
     return set_err(h, LBM_ERR_STATE, "unknown device error word " + std::to_string(err));
 }
 
+// vector tiles of `B` threads: B / (nx/4) whole x-rows of one z-slice
+void set_vector_block(lbm_handle* h, int B) {
+    const int RT = h->n[0] / 4;
+    h->vblock = B;
+    h->vrows = std::max(1, std::min(B / RT, h->n[1]));
+    h->vnt1 = (h->n[1] + h->vrows - 1) / h->vrows;
+    h->vtiles = (long long)h->vnt1 * h->n[2];
+}
+
 // CTA tile: full x-rows up to 256 nodes (x-wrap stays inside the CTA)
 void choose_tiles(lbm_handle* h) {
     GridDesc& g = h->g;
@@ -763,27 +772,27 @@ void choose_tiles(lbm_handle* h) {
     for (int k = 0; k < 3; ++k) g.nt[k] = (h->n[k] + g.t[k] - 1) / g.t[k];
     g.N = h->N;
     g.ntiles = (long long)g.nt[0] * g.nt[1] * g.nt[2];
-    // vector tiles: whole x-rows, 4 nodes per thread.  Rows of up to 256
-    // nodes take kTickBlock-thread CTAs (the persistent tick kernel's size);
-    // wider rows the CTA size (up to 512) that leaves the fewest idle threads.
+    // vector tiles: whole x-rows, 4 nodes per thread, in the CTA size that
+    // leaves the fewest idle threads (kTickBlock on a tie: 96 threads for rows
+    // of 96 or 192 nodes, 64 for rows of 4*2^k <= 256).  The persistent tick
+    // kernel and batch queues run kTickBlock-thread tiles: set_vector_block.
     h->vrows = h->vnt1 = h->vblock = 0;
     h->vtiles = 0;
     if (h->n[0] % 4 == 0 && h->n[0] / 4 <= 512) {
         const int RT = h->n[0] / 4;
         double best = -1.0;
+        int pick = 0;
         for (int B : kBulkBlocks) {
             if (B < RT) continue;
             const int rows = std::min(B / RT, h->n[1]);
             const double use = (double)(rows * RT) / B;
-            if (use > best + 1e-9) {
-                best = use;
-                h->vblock = B;
+            if (use > best + 1e-9 || (use > best - 1e-9 && B == kTickBlock)) {
+                best = std::max(best, use);
+                pick = B;
             }
         }
-        if (RT <= kTickBlock) h->vblock = kTickBlock;
-        h->vrows = std::max(1, std::min(h->vblock / RT, h->n[1]));
-        h->vnt1 = (h->n[1] + h->vrows - 1) / h->vrows;
-        h->vtiles = (long long)h->vnt1 * h->n[2];
+        if (h->schedule == LBM_SCHEDULE_PERSISTENT && RT <= kTickBlock) pick = kTickBlock;
+        set_vector_block(h, pick);
     }
 }
 
@@ -1539,14 +1548,12 @@ int lbm_set_bulk_kernel(lbm_handle* h, int32_t kind, int32_t threads, int32_t st
         return set_err(h, LBM_ERR_UNSUPPORTED, "the vector bulk kernel does not apply to this model");
     if (kind == LBM_BULK_VECTOR && threads != 0) {  // CTA size of the vector kernel (tiles of whole x-rows)
         const int RT = h->n[0] / 4;
-        if ((threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512) || threads < RT ||
-            threads % RT != 0 || h->schedule == LBM_SCHEDULE_PERSISTENT)
+        if ((threads != 32 && threads != 64 && threads != 96 && threads != 128 && threads != 256 && threads != 512) ||
+            threads < RT || threads % RT != 0 || h->schedule == LBM_SCHEDULE_PERSISTENT)
             return set_err(h, LBM_ERR_UNSUPPORTED,
-                           "vector kernel CTAs hold whole x-rows: 32..512 threads, a multiple of nx/4 (stream schedule)");
-        h->vblock = threads;
-        h->vrows = std::max(1, std::min(threads / RT, h->n[1]));
-        h->vnt1 = (h->n[1] + h->vrows - 1) / h->vrows;
-        h->vtiles = (long long)h->vnt1 * h->n[2];
+                           "vector kernel CTAs hold whole x-rows: 32, 64, 96, 128, 256 or 512 threads, a multiple of "
+                           "nx/4 (stream schedule)");
+        set_vector_block(h, threads);
     }
     if (kind != LBM_BULK_VECTOR) {
         TmaShape sh{};
@@ -1675,6 +1682,24 @@ int lbm_get_stress(lbm_handle* h, double* sigma) {
     CUDA_TRY(h, cudaGetLastError());
     CUDA_TRY(h, cudaMemcpyAsync(sigma, c.stress, nb, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm_get_totals(lbm_handle* h, double* mass, double* momentum) {
+    if (!h) return set_err(h, LBM_ERR_INVALID, "null handle");
+    BIND(h);
+    const long long nb = (h->N + kTotBlock - 1) / kTotBlock;
+    int rc = ensure_tmp(h, sizeof(double) * (4 * nb + 4));
+    if (rc) return rc;
+    CodecArgs c = codec_args(h);
+    h->ops.totals(c, h->d_tmp, h->d_tmp + 4 * nb, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    double t[4];
+    CUDA_TRY(h, cudaMemcpyAsync(t, h->d_tmp + 4 * nb, sizeof(t), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (mass) *mass = t[0];
+    if (momentum)
+        for (int k = 0; k < 3; ++k) momentum[k] = k < h->dims ? t[1 + k] : 0.0;
     return LBM_OK;
 }
 
@@ -2514,6 +2539,7 @@ int lbm_batch_create(int32_t n, const lbm_config* cfgs, const int32_t* nparticle
             return bset_err(nullptr, rc, m);
         }
         h->in_batch = true;
+        if (use_vector_bulk(h) && h->n[0] / 4 <= kTickBlock) set_vector_block(h, kTickBlock);  // queue tiles
         b->reps.push_back(h);
         const int np = nparticles ? nparticles[r] : 0;
         for (int p = 0; p < np; ++p, ++k) {

@@ -25,7 +25,8 @@ struct Ops {
     void (*decode)(const CodecArgs&, cudaStream_t);
     void (*macro)(const CodecArgs&, cudaStream_t);
     void (*stress)(const CodecArgs&, cudaStream_t);
-    void (*check)(const CodecArgs&, int*, cudaStream_t);
+    // global FP64 sums: rho and rho u into out[4] (part: one slot of 4 per kTotBlock cells)
+    void (*totals)(const CodecArgs&, double* part, double* out, cudaStream_t);
     void (*init)(const InitArgs&, cudaStream_t);
     void (*mask)(const MaskArgs&, cudaStream_t);
     // vector bulk pass over all tiles, CTAs of `block` threads (64..512); null for FP64
@@ -49,7 +50,7 @@ struct Ops {
     const void* bulk_tma_fn_sr;
 };
 
-constexpr int kBulkBlocks[4] = {64, 128, 256, 512};  // CTA sizes of the vector bulk kernel (and 32 on request)
+constexpr int kBulkBlocks[5] = {64, 96, 128, 256, 512};  // CTA sizes of the vector bulk kernel (and 32 on request)
 
 inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
@@ -85,6 +86,7 @@ struct OpsImpl {
         const unsigned g = (unsigned)tiles;
         if (block <= 32) k_bulk_v4<L, ST, TRT, 32, SR><<<g, 32, 0, s>>>(a);
         else if (block <= 64) k_bulk_v4<L, ST, TRT, 64, SR><<<g, 64, 0, s>>>(a);
+        else if (block <= 96) k_bulk_v4<L, ST, TRT, 96, SR><<<g, 96, 0, s>>>(a);
         else if (block <= 128) k_bulk_v4<L, ST, TRT, 128, SR><<<g, 128, 0, s>>>(a);
         else if (block <= 256) k_bulk_v4<L, ST, TRT, 256, SR><<<g, 256, 0, s>>>(a);
         else k_bulk_v4<L, ST, TRT, 512, SR><<<g, 512, 0, s>>>(a);
@@ -138,8 +140,10 @@ struct OpsImpl {
     static void decode(const CodecArgs& a, cudaStream_t s) { k_decode<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void macro(const CodecArgs& a, cudaStream_t s) { k_macro<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void stress(const CodecArgs& a, cudaStream_t s) { k_stress<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
-    static void check(const CodecArgs& a, int* bad, cudaStream_t s) {
-        k_check<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a, bad);
+    static void totals(const CodecArgs& a, double* part, double* out, cudaStream_t s) {
+        const unsigned nb = blocks_for(a.N, kTotBlock);
+        k_totals<L, ST><<<nb, kTotBlock, 0, s>>>(a, part);
+        k_totals_final<<<1, kTotBlock, 0, s>>>(part, (long long)nb, out);
     }
     static void init(const InitArgs& a, cudaStream_t s) { k_init<L, ST><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
     static void mask(const MaskArgs& a, cudaStream_t s) { k_mask<L::D><<<blocks_for(a.N, 256), 256, 0, s>>>(a); }
@@ -153,7 +157,7 @@ struct OpsImpl {
         o.decode = decode;
         o.macro = macro;
         o.stress = stress;
-        o.check = check;
+        o.totals = totals;
         o.init = init;
         o.mask = mask;
         o.bulk_v4 = ST == ST_F64 ? nullptr : bulk_v4;

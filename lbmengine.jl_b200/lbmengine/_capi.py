@@ -201,6 +201,7 @@ PROTOTYPES = [
     ("lbm_get_fields", C.c_int, [C.c_void_p, _dp, _dp]),
     ("lbm_get_distributions", C.c_int, [C.c_void_p, _dp]),
     ("lbm_get_stress", C.c_int, [C.c_void_p, _dp]),
+    ("lbm_get_totals", C.c_int, [C.c_void_p, _dp, _dp]),
     ("lbm_record_trajectories", C.c_int, [C.c_void_p, C.c_int64]),
     ("lbm_read_trajectories", C.c_int, [C.c_void_p, _dp, C.c_int64, C.POINTER(C.c_int64)]),
     ("lbm_write_fluid_csv", C.c_int, [C.c_void_p, C.c_char_p]),

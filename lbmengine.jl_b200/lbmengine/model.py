@@ -119,6 +119,13 @@ class LBMmodel:
         flat = np.ascontiguousarray(f.ravel(order="F"))
         self._check(self._lib.lbm_set_distributions(self._h, flat.ctypes.data_as(capi._dp)))
 
+    def totals(self):
+        """(sum of rho, sum of rho u): global FP64 sums on the device (lbm_get_totals)."""
+        m = C.c_double()
+        p = (C.c_double * 3)()
+        self._check(self._lib.lbm_get_totals(self._h, C.byref(m), p))
+        return m.value, np.array(p[:self._dims])
+
     def viscous_stress_tensor(self) -> np.ndarray:
         """viscousStressTensor(model) (src/cpu/fluids.jl:507-520): array (N..., d, d)."""
         d = self._dims

@@ -1,6 +1,6 @@
 """Generate the golden fixtures under tests/golden/.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <checkout of LBMengine.jl>
 
 1. velocity_sets.json — the D2Q9/D3Q15/D3Q19/D3Q27 tables (direction order,
    lattice vectors, weights) read as TEXT from the reference's
@@ -130,7 +130,7 @@ def make_oracle_small():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of a checkout of david16correa/LBMengine.jl")
     ap.add_argument("--skip-oracle", action="store_true")
     a = ap.parse_args()
     sets = make_velocity_sets(a.reference)

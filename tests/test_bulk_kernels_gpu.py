@@ -1,9 +1,9 @@
 """The bulk stream-collide kernels give bit-identical ticks.
 
-The vector kernel and the TMA kernel (bulk copies through a shared-memory
-ring) run the same collision on the same values and store with the same
-rounding, so whole runs must agree bit for bit, in every storage format and
-launch shape.  The FP16/BF16 stores round stochastically with a dither that
+The vector kernel (in every CTA shape) and the TMA kernel (bulk copies
+through a shared-memory ring) run the same collision on the same values and
+store with the same rounding, so whole runs must agree bit for bit, in every
+storage format and launch shape.  The FP16/BF16 stores round stochastically with a dither that
 is a function of (cell, direction, value) only, so results do not depend on
 how the ticks are split into calls either.
 """
@@ -90,3 +90,66 @@ def test_dithered_rounding_does_not_depend_on_call_chunking(lib, storage):
     for _ in range(23):
         assert lib.lbm_step_noalloc(c.handle, 1) == 0
     np.testing.assert_array_equal(a.distributions, c.distributions)
+
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("vel,nx,threads", [("D3Q19", 128, 128), ("D3Q19", 64, 128), ("D3Q19", 32, 256),
+                                            ("D3Q27", 32, 128), ("D2Q9", 64, 256), ("D2Q9", 16, 32)])
+@pytest.mark.parametrize("rounding", ["stochastic", "nearest"])
+def test_vector_kernel_cta_shapes_agree(lib, storage, vel, nx, threads, rounding):
+    """The default shape (64 threads) against another CTA size."""
+    if storage == "f32" and rounding == "nearest":
+        pytest.skip("FP32 stores do not round")
+    d = 2 if vel == "D2Q9" else 3
+    ms = []
+    for t in (0, threads):
+        h = nx // 2
+        res = config.resolve_model(dims=d, velocities=vel, collisionModel="trt", kineticParameter=3 / 16,
+                                   latticeParameter=1.0, relaxationTimeRatio=0.7,
+                                   xlims=(-float(h), float(nx - h - 1)), ylims=(-8.0, 7.0), zlims=(-6.0, 5.0),
+                                   forceDensity=[1e-5] + [0.0] * (d - 1), storage=storage, rounding=rounding)
+        m = M.LBMmodel(res)
+        M._add(m, config.resolve_squirmer(d, radius=4.0, position=[0.3, -0.2, 0.1][:d], swimmingSpeed=1e-3,
+                                          beta=-3.0, swimmingDirection=[0.6, 0.0, 0.8] if d == 3 else [0.6, 0.8],
+                                          coupleForces=True, coupleTorques=True))
+        inf = _kernel(m, _capi.LBM_BULK_VECTOR, t)
+        assert inf.bulk_threads == (threads if t else 64)
+        ms.append(m)
+    ref, other = ms
+    for n in (1, 6, 17):
+        ref.step(n)
+        other.step(n)
+        np.testing.assert_array_equal(other.distributions, ref.distributions)
+    for a, b in zip(other.particle_states(), ref.particle_states()):
+        assert list(a.position) == list(b.position) and list(a.last_force) == list(b.last_force)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("vel,nx", [("D3Q19", 96), ("D3Q19", 192), ("D2Q9", 192), ("D2Q9", 48)])
+def test_96_thread_ctas_against_the_oracle(lib, oracle_mod, storage, vel, nx):
+    """Rows of 96 or 192 nodes (24 or 48 threads) fill 96-thread CTAs without
+    idle threads; checked against the FP64 oracle with the parity tolerances
+    (FP16 density to 3e-5)."""
+    from test_parity_gpu import TOL, compare_state
+    d = 2 if vel == "D2Q9" else 3
+    h = nx // 2
+    model = dict(dims=d, velocities=vel, collisionModel="trt", kineticParameter=3 / 16, latticeParameter=1.0,
+                 relaxationTimeRatio=0.7, xlims=(-float(h), float(nx - h - 1)), ylims=(-16.0, 15.0),
+                 forceDensity=[1e-5] + [0.0] * (d - 1))
+    if d == 3:
+        model["zlims"] = (-16.0, 15.0)
+    sq = dict(radius=4.5, position=[0.3, -0.2, 0.1][:d], swimmingSpeed=5e-4 / 1.5 * 4, beta=-5.0,
+              swimmingDirection=[0.6, 0.0, 0.8] if d == 3 else [0.6, 0.8], coupleForces=True, coupleTorques=True)
+    res = config.resolve_model(**model, storage=storage)
+    m = M.LBMmodel(res)
+    orc = oracle_mod.OracleModel(res)
+    for tgt in (m, orc):
+        prm = config.resolve_squirmer(d, **sq)
+        M._add(tgt, prm) if tgt is m else tgt.add_particle(prm)
+    inf = m.info()
+    assert inf.bulk_kernel == _capi.LBM_BULK_VECTOR and inf.bulk_threads == 96
+    m.step(40)
+    orc.step(40)
+    tol = dict(TOL[storage], field=3e-5) if storage == "f16" else TOL[storage]
+    compare_state(res, m, orc, tol, f"{vel} nx={nx} {storage}")

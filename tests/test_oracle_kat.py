@@ -268,3 +268,38 @@ def test_rules_share_the_fluid_step(oracle_mod):
     kw = dict(_MODEL_2D, walledDimensions=[2])
     g, c = _rules_pair(oracle_mod, kw, [], 60)
     np.testing.assert_array_equal(g.distributions(), c.distributions())
+
+
+def test_parity_assertions_catch_a_flipped_torque():
+    """compare_state (the GPU parity check) fails when one torque component of
+    the checked model has the wrong sign; the mistake is planted in stand-in
+    state objects on the CPU, not in any GPU code."""
+    from types import SimpleNamespace
+
+    import test_parity_gpu as tp
+
+    def state(torque):
+        return SimpleNamespace(position=[0.1, 0.2, 0.3], velocity=[1e-4, 0.0, 0.0], angular_velocity=[0.0, 0.0, 1e-6],
+                               swimming_direction=[1.0, 0.0, 0.0], last_force=[2e-5, 1e-5, 0.0],
+                               last_torque=torque, radius=4.0)
+
+    class Fake:
+        def __init__(self, torque):
+            self.massDensity = np.ones((2, 2, 2))
+            self.fluidVelocity = np.full((2, 2, 2, 3), 1e-4)
+            self.s = [state(torque)]
+
+        def particle_states(self):
+            return self.s
+
+        def fields(self):
+            return np.ones(8), np.full((3, 8), 1e-4)
+
+        def particles(self):
+            return self.s
+
+    res = SimpleNamespace(dims=3)
+    good = [3e-5, -2e-5, 1e-5]
+    tp.compare_state(res, Fake(good), Fake(good), tp.TOL["f64"], "same")
+    with pytest.raises(AssertionError, match="torque"):
+        tp.compare_state(res, Fake([3e-5, 2e-5, 1e-5]), Fake(good), tp.TOL["f64"], "flipped")

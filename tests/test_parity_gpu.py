@@ -193,3 +193,35 @@ def test_viscous_stress_tensor(lib, oracle_mod, name, storage):
             tol = 1e-9 if storage == "f64" else 2e-3
             assert np.max(np.abs(g - so[a, b])) <= tol * scale, (a, b)
     np.testing.assert_allclose(sg[..., 0, 1], sg[..., 1, 0], rtol=0, atol=1e-15 * scale + 1e-300)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16"])
+def test_device_totals_conserve_and_match_the_oracle(lib, oracle_mod, storage):
+    """Global FP64 sums on the device (lbm_get_totals): equal to the sums of the
+    read-back fields and to the oracle's.  With a particle the grid's total
+    mass is not conserved, in the reference either: particle interiors keep
+    streaming, and the populations they push into fluid nodes are replaced by
+    the bounce-back (src/gpu/fluids.jl:154-165).  Without one, mass is
+    conserved and momentum grows by the body force, N F per tick."""
+    case = CASES["d3q19_trt_guo_squirmer"]
+    res, gpu, orc = build_pair(case, storage=storage, oracle_mod=oracle_mod)
+    gpu.step(20)
+    orc.step(20)
+    m1, p1 = gpu.totals()
+    rho = gpu.massDensity.ravel(order="F")
+    u = gpu.fluidVelocity.reshape(-1, 3, order="F")
+    assert abs(m1 - rho.sum()) <= 1e-12 * m1
+    np.testing.assert_allclose(p1, (rho[:, None] * u).sum(0), rtol=1e-9, atol=1e-12)
+    rho_o, u_o = orc.fields()
+    assert abs(m1 - rho_o.sum()) <= (1e-11 if storage == "f64" else 1e-5) * m1
+    po = (rho_o[None, :] * u_o).sum(1)
+    np.testing.assert_allclose(p1, po, rtol=0, atol=(1e-11 if storage == "f64" else 1e-3) * np.abs(po).max())
+    # no particle: mass conserved, momentum grows by exactly N F per tick
+    res2, g2, _ = build_pair(dict(case, particles=[]), storage=storage)
+    m_a, q0 = g2.totals()
+    g2.step(10)
+    m_b, q1 = g2.totals()
+    assert abs(m_b - m_a) <= (1e-12 if storage == "f64" else 1e-7) * m_a
+    n = np.prod(res2.shape)
+    tol = {"f64": 1e-12, "f32": 1e-6, "f16": 3e-5}[storage] * 10 * n * 1e-5
+    np.testing.assert_allclose(q1 - q0, [10 * n * 1e-5, 0.0, 0.0], rtol=0, atol=tol)
