@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(512, 1) k_bulk_tma(const StepArgs a, const int
         report_density(valid && bad, a.err);
         constexpr bool sr = SR && Store<ST>::bytes == 2;
         unsigned dw[4];
-        if (sr) dither_words<Store<ST>::drop>(group_dither((int)(x0 + nx * (y + (long long)ny * z)), g[0][1], g[0][2],
+        if (sr) rs_words(group_dither((int)(x0 + nx * (y + (long long)ny * z)), g[0][1], g[0][2],
                                                            g[0][3]), dw);
         const unsigned* dither = sr ? dw : nullptr;
         const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};

@@ -544,14 +544,14 @@ template <> struct Vec4<ST_F16> {
     static __device__ __forceinline__ void load(const void* base, int cell0, float* v) {
         unpack(__ldcs(reinterpret_cast<const uint2*>(static_cast<const __half*>(base) + cell0)), v);
     }
-    // rounding to nearest (dither null) or stochastic with the group's dither
-    // words (storage.cuh): cell k of direction dir adds word (k + dir) mod 4
+    // rounding to nearest (dither null) or stochastic with the group's random
+    // words (storage.cuh): cells (2p, 2p+1) of direction dir take word (dir + 2p) mod 4
     static __device__ __forceinline__ void store(void* base, int cell0, int dir, float a0, float a1, float a2,
                                                  float a3, const unsigned* dither) {
         uint2 q;
         if (dither) {
-            q.x = pack_half2_rz(add_dither(a0, dither[dir & 3]), add_dither(a1, dither[(dir + 1) & 3]));
-            q.y = pack_half2_rz(add_dither(a2, dither[(dir + 2) & 3]), add_dither(a3, dither[(dir + 3) & 3]));
+            q.x = pack_half2_rs(a0, a1, dither[dir & 3]);
+            q.y = pack_half2_rs(a2, a3, dither[(dir + 2) & 3]);
         } else {
             const __half2 lo = __floats2half2_rn(a0, a1);
             const __half2 hi = __floats2half2_rn(a2, a3);
@@ -575,8 +575,8 @@ template <> struct Vec4<ST_BF16> {
                                                  float a3, const unsigned* dither) {
         uint2 q;
         if (dither) {
-            q.x = pack_bf162_rz(add_dither(a0, dither[dir & 3]), add_dither(a1, dither[(dir + 1) & 3]));
-            q.y = pack_bf162_rz(add_dither(a2, dither[(dir + 2) & 3]), add_dither(a3, dither[(dir + 3) & 3]));
+            q.x = pack_bf162_rs(a0, a1, dither[dir & 3]);
+            q.y = pack_bf162_rs(a2, a3, dither[(dir + 2) & 3]);
         } else {
             const __nv_bfloat162 lo = __floats2bfloat162_rn(a0, a1);
             const __nv_bfloat162 hi = __floats2bfloat162_rn(a2, a3);
@@ -667,7 +667,7 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
     report_density(valid && bad, a.err);
     constexpr bool sr = SR && Store<ST>::bytes == 2;
     unsigned dw[4];
-    if (sr) dither_words<Store<ST>::drop>(group_dither(cell0, g[0][1], g[0][2], g[0][3]), dw);
+    if (sr) rs_words(group_dither(cell0, g[0][1], g[0][2], g[0][3]), dw);
     const unsigned* dither = sr ? dw : nullptr;
     // the value of each +-x direction that leaves this thread's 4-node segment
     if (row < a.vrows) {
@@ -692,11 +692,11 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
 // memory-bound, and up to 96 (20 warps per SM) with 2-byte storage, whose
 // conversions make it issue-bound as well: the extra warps took its 128^3
 // pass from 28.4 to 26.9 us, with no change for FP32.
-// With stochastic rounding the 2-byte kernels keep the dither word and its
-// arithmetic in registers: 18 warps per SM (112 registers) instead of 20.
+// Stochastic rounding (one conversion per two values with the group's
+// random words) fits the same 96 registers.
 template <class L, int ST = ST_F32, bool SR = false>
 constexpr int bulk_threads_per_sm() {
-    return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? (SR ? 576 : 640) : 512);
+    return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? 640 : 512);
 }
 
 // the vector bulk pass over all tiles, one CTA of B threads per tile

@@ -39,15 +39,14 @@ __device__ __forceinline__ float round_dither(float v, unsigned key, unsigned mu
     return __uint_as_float((b + (h >> (32 - DROP))) & M);
 }
 
-// Dither of a thread's group of four cells (the vector bulk kernels): one
-// well-mixed 32-bit word from the group's first cell and the kept bits of
+// Random bits of a thread's group of four cells (the vector bulk kernels):
+// one well-mixed 32-bit word from the group's first cell and the kept bits of
 // three of its post-collision values (which change from tick to tick as the
-// flow evolves), spread into four independent words (dither_words).  The
-// value of direction i of cell k adds word (k + i) mod 4 to its FP32 bits and
-// is converted rounding toward zero: the discarded fraction is rounded up
-// exactly when it exceeds the dither.  For every (k, i) the dither is uniform
-// over the nodes of a flow, so the rounding is unbiased, at one integer
-// addition per value.
+// flow evolves), spread into four independent 32-bit words (rs_words).  The
+// pair of cells (2p, 2p+1) of direction i is converted by the hardware's
+// stochastic-rounding conversion (cvt.rs) with word (i + 2p) mod 4 as its
+// random bits.  For every (p, i) the word is uniform over the nodes of a flow,
+// so the rounding is unbiased, at one instruction per two values.
 __device__ __forceinline__ unsigned group_dither(int cell0, float v1, float v2, float v3) {
     unsigned x = ((__float_as_uint(v1) ^ __float_as_uint(v2) ^ __float_as_uint(v3)) & 0xFFFFE000u) ^
                  ((unsigned)cell0 * kDitherCell);
@@ -58,31 +57,32 @@ __device__ __forceinline__ unsigned group_dither(int cell0, float v1, float v2, 
     return x;
 }
 
-// four independent dither words of DROP bits from a group's word
-template <int DROP>
-__device__ __forceinline__ void dither_words(unsigned x, unsigned* w) {
+// four independent 32-bit words from a group's word (multiply-xorshift steps)
+__device__ __forceinline__ void rs_words(unsigned x, unsigned* w) {
     unsigned y = x * 0x85EBCA6Bu;
     y ^= y >> 13;
-    constexpr unsigned M = (1u << DROP) - 1u;
-    w[0] = x & M;
-    w[1] = (x >> 16) & M;
-    w[2] = y & M;
-    w[3] = (y >> 16) & M;
+    unsigned z = y * 0xC2B2AE35u;
+    z ^= z >> 16;
+    unsigned u = z * 0x27D4EB2Fu;
+    u ^= u >> 15;
+    w[0] = x;
+    w[1] = y;
+    w[2] = z;
+    w[3] = u;
 }
 
-// v with a dither added to its bits below the kept ones (a conversion toward
-// zero then rounds it stochastically)
-__device__ __forceinline__ float add_dither(float v, unsigned d) { return __uint_as_float(__float_as_uint(v) + d); }
-
-// two floats to a packed half2 / bfloat162 rounding toward zero (lo in the low half)
-__device__ __forceinline__ unsigned pack_half2_rz(float lo, float hi) {
+// two floats to a packed half2 / bfloat162 (lo in the low half), rounded
+// stochastically by the conversion with the random bits `rbits` (sm_100a);
+// finite values saturate at the largest finite value, as rounding toward
+// zero does
+__device__ __forceinline__ unsigned pack_half2_rs(float lo, float hi, unsigned rbits) {
     unsigned r;
-    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
     return r;
 }
-__device__ __forceinline__ unsigned pack_bf162_rz(float lo, float hi) {
+__device__ __forceinline__ unsigned pack_bf162_rs(float lo, float hi, unsigned rbits) {
     unsigned r;
-    asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
     return r;
 }
 
