@@ -720,11 +720,14 @@ int build_graph(lbm_handle* h, int start, int size_idx) {
     return LBM_OK;
 }
 
-// every graph of the current profiling level, for both starting buffers, so
-// that no call after the first captures or instantiates
-int ensure_graphs(lbm_handle* h) {
+// The graphs a call of `nsteps` ticks can launch: every size up to nsteps, for
+// both starting buffers, built before the call's first launch (and before its
+// profiling start event).  A short first call does not pay for the 64-tick
+// graphs; a later, longer call builds them once, before its own launches.
+int ensure_graphs(lbm_handle* h, int64_t nsteps) {
     for (int start = 0; start < 2; ++start)
         for (int k = 0; k < 4; ++k) {
+            if (kModelGraphSizes[k] > nsteps) continue;
             const int rc = build_graph(h, start, k);
             if (rc) return rc;
         }
@@ -1447,7 +1450,7 @@ int lbm_step(lbm_handle* h, int64_t nsteps) {
         if (rc) return rc;
     }
     if (nsteps > 0) {
-        const int rc = ensure_graphs(h);
+        const int rc = ensure_graphs(h, nsteps);
         if (rc) return rc;
     }
     if (h->profiling) CUDA_TRY(h, cudaEventRecord(h->t_begin, h->stream));

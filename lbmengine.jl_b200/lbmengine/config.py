@@ -153,7 +153,8 @@ def resolve_model(massDensity=DEFAULT, fluidVelocity=DEFAULT, velocities=DEFAULT
                                       "Please use the cpu modules instead.")
         wall = wall_nodes(shape, walledDimensions)
         schemes.append("bounceBack")
-    grids = np.meshgrid(*axes, indexing="ij")
+    # coordinate grids, only for the wall functions that are evaluated on them
+    grids = np.meshgrid(*axes, indexing="ij") if (walls is not DEFAULT or movingWalls is not DEFAULT) else None
     if walls is not DEFAULT:
         _assert(callable(walls), "walls must be a function!")
         new = np.vectorize(walls, otypes=[object])(*grids)

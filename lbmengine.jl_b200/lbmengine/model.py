@@ -89,21 +89,28 @@ class LBMmodel:
     def time(self) -> float:
         return float(self.info().time)
 
-    def _fields(self):
-        rho = np.empty(self._cells, dtype=np.float64)
-        u = np.empty(self._cells * self._dims, dtype=np.float64)
-        self._check(self._lib.lbm_get_fields(self._h, rho.ctypes.data_as(capi._dp), u.ctypes.data_as(capi._dp)))
-        return rho, u
+    def read_fields(self, rho=None, u=None) -> None:
+        """Write rho (shape N...) and u (N..., d) into caller-owned float64
+        arrays in column-major order (a Julia array's layout, e.g. numpy
+        arrays made with order="F", or pinned host memory); either may be None."""
+        for a, shape in ((rho, self._shape), (u, self._shape + (self._dims,))):
+            if a is not None and (a.dtype != np.float64 or a.shape != shape or not a.flags.f_contiguous
+                                  or not a.flags.writeable):
+                raise ValueError(f"expected a writeable column-major float64 array of shape {shape}")
+        self._check(self._lib.lbm_get_fields(self._h, None if rho is None else rho.ctypes.data_as(capi._dp),
+                                             None if u is None else u.ctypes.data_as(capi._dp)))
 
     @property
     def massDensity(self) -> np.ndarray:
-        rho, _ = self._fields()
-        return rho.reshape(self._shape, order="F")
+        rho = np.empty(self._shape, dtype=np.float64, order="F")
+        self.read_fields(rho=rho)
+        return rho
 
     @property
     def fluidVelocity(self) -> np.ndarray:
-        _, u = self._fields()
-        return u.reshape(self._shape + (self._dims,), order="F")
+        u = np.empty(self._shape + (self._dims,), dtype=np.float64, order="F")
+        self.read_fields(u=u)
+        return u
 
     @property
     def distributions(self) -> np.ndarray:
