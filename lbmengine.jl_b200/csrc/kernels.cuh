@@ -693,10 +693,13 @@ __device__ __forceinline__ void bulk_v4_tile(const StepArgs& a, long long tile, 
 // conversions make it issue-bound as well: the extra warps took its 128^3
 // pass from 28.4 to 26.9 us, with no change for FP32.
 // Stochastic rounding (one conversion per two values with the group's
-// random words) fits the same 96 registers.
+// random words) fits the same 96 registers.  A D3Q27 thread holds 108
+// populations: 12 warps per SM (168 registers) with FP32/FP64 storage, 14
+// (144) with 2-byte storage, so that neither spills.
 template <class L, int ST = ST_F32, bool SR = false>
 constexpr int bulk_threads_per_sm() {
-    return L::Q <= 9 ? 1024 : (Store<ST>::bytes == 2 ? 640 : 512);
+    return L::Q <= 9 ? 1024
+                     : (L::Q > 19 ? (Store<ST>::bytes == 2 ? 448 : 384) : (Store<ST>::bytes == 2 ? 640 : 512));
 }
 
 // the vector bulk pass over all tiles, one CTA of B threads per tile
