@@ -332,6 +332,15 @@ def run_ours(args):
     ring = lbm_output.RING_TICKS
     rows = np.empty(ring * 9, dtype=np.float64)
     got = __import__("ctypes").c_int64()
+    # one untimed pass of the same calls (2 ticks): the process's first use of
+    # each of them (kernel modules, pinned transfers) is not the steady state
+    mw = lbm_model.LBMmodel(config.resolve_model(**dict(mkw, massDensity=rho0, fluidVelocity=u0)))
+    lbm_model._add(mw, config.resolve_squirmer(3, **skw))
+    mw._check(lib.lbm_record_trajectories(mw.handle, ring))
+    mw.step(2)
+    mw._check(lib.lbm_read_trajectories(mw.handle, rows.ctypes.data_as(_capi._dp), 2, __import__("ctypes").byref(got)))
+    mw.read_fields(rho_out, u_out)
+    mw.close()
     barrier(dist)
     t0 = time.perf_counter()
     m2 = lbm_model.LBMmodel(config.resolve_model(**dict(mkw, massDensity=rho0, fluidVelocity=u0)))
@@ -356,7 +365,8 @@ def run_ours(args):
            "path": "modelInit with pinned column-major host rho/u (lbm_create) + addSquirmer + LBMpropagate in "
                    f"blocks of up to {ring} ticks, each block's per-tick particle states read from the device "
                    "trajectory ring (lbm_read_trajectories), then massDensity/fluidVelocity into pinned host "
-                   "arrays (lbm_get_fields); host wall clock, including the graph builds of the first call"}
+                   "arrays (lbm_get_fields); host wall clock, including the model's graph builds, after one "
+                   "untimed 2-tick pass of the same calls"}
     del keep
 
     cpu = None

@@ -720,17 +720,26 @@ int build_graph(lbm_handle* h, int start, int size_idx) {
     return LBM_OK;
 }
 
-// The graphs a call of `nsteps` ticks can launch: every size up to nsteps, for
-// both starting buffers, built before the call's first launch (and before its
-// profiling start event).  A short first call does not pay for the 64-tick
-// graphs; a later, longer call builds them once, before its own launches.
+// The graphs a call of `nsteps` ticks launches (the largest sizes first, as
+// lbm_step does, from the current buffer), built before the call's first
+// launch and before its profiling start event: a call pays only for the
+// graphs it is the first to need, never in the middle of its launches.
 int ensure_graphs(lbm_handle* h, int64_t nsteps) {
-    for (int start = 0; start < 2; ++start)
-        for (int k = 0; k < 4; ++k) {
-            if (kModelGraphSizes[k] > nsteps) continue;
-            const int rc = build_graph(h, start, k);
-            if (rc) return rc;
+    static_assert(kModelGraphSizes[0] % 2 == 0, "the largest graph must leave the buffer unchanged");
+    int64_t done = 0;
+    int cur = h->cur;
+    while (done < nsteps) {
+        int k = 0;
+        while (kModelGraphSizes[k] > nsteps - done) ++k;
+        const int rc = build_graph(h, cur, k);
+        if (rc) return rc;
+        if (k == 0) {  // the largest graph repeats without changing the buffer
+            done += (nsteps - done) / kModelGraphSizes[0] * kModelGraphSizes[0];
+            continue;
         }
+        done += kModelGraphSizes[k];
+        if (kModelGraphSizes[k] & 1) cur = 1 - cur;
+    }
     return LBM_OK;
 }
 
