@@ -9,6 +9,10 @@
 //   f^{n+1}_j(x) = f*_i(x) + 6 w_j rho^n(x) c_j.u_p(x-c_j),  i = opp(j),
 //                  for the particle's boundary links (x fluid, x - c_j solid)
 //   F = sum_links coeff (f*_i + f^{n+1}_j) c_i,  T = sum_links coeff (f*_i + f^{n+1}_j) (x - R) x c_i
+// Walls (static, fluids.jl:147-174): wall nodes hold f = 0 after streaming,
+// and a fluid node x whose source x - c_j is a wall node gets
+//   f^{n+1}_j(x) = f*_i(x) + 6 w_j rho^n(x) c_j.u_w(x - c_j)  (+ the particles' Ladd terms),
+// which the momentum exchange of a particle with the same link also sees.
 // The solid masks are held as the forward run computed them (their
 // derivative is zero almost everywhere).  Adjoint populations are FP64 and
 // in f units; the forward populations are read in their storage format and
@@ -69,6 +73,8 @@ struct AdjArgs {
     const double* coord[3];
     const ParticleDev* part;  // the particle at tick n (one particle)
     const int2* ivl;
+    const unsigned char* wall;  // wall nodes (null: no walls)
+    const double* uw;           // wall velocity [d][N] (null: static walls)
     int has_part;
     int pad;
     double rho0, inv_scale;  // stored g' = S (f/w - rho0)
@@ -268,32 +274,47 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(const AdjArgs a) {
 
         // 1. adjoint of the post-collision populations: transposed streaming
         const ParticleDev& P = *a.part;
+        const bool wx = a.wall && a.wall[cell];  // a wall node: everything it streams is discarded
         const bool sx = a.has_part && solid_at(P, a.ivl, x, y, z);
         double ls[L::Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const int tx = wrap_idx(x + L::cx(i), nx), ty = wrap_idx(y + L::cy(i), ny), tz = wrap_idx(z + L::cz(i), nz);
-            const bool slot = sx && !solid_at(P, a.ivl, tx, ty, tz);  // (x + c_i, i) was overwritten by the fix-up
-            ls[i] = slot ? 0.0 : a.lam_in[i * N + tx + (long long)nx * (ty + (long long)ny * tz)];
+            const long long t = tx + (long long)nx * (ty + (long long)ny * tz);
+            // (x + c_i, i) was overwritten by the fix-up (a particle's or a wall's link slot), or zeroed (a wall node)
+            const bool slot = wx || (sx && !solid_at(P, a.ivl, tx, ty, tz)) || (a.wall && a.wall[t]);
+            ls[i] = slot ? 0.0 : a.lam_in[i * N + t];
         }
-        // 2. link terms of a fluid node: bounce-back, Ladd and momentum exchange
+        // 2. link terms of a fluid node: bounce-back, moving walls, Ladd and momentum exchange
         double mu_rho = 0.0;
-        if (a.has_part && !sx) {
+        if (!wx && !sx && (a.has_part || a.wall)) {
             const double X[3] = {a.coord[0][x], a.coord[1][y], D == 3 ? a.coord[2][z] : 0.0};
             for (int j = 1; j < Q; ++j) {
                 const int i = L::opp(j);
                 const int sxx = wrap_idx(x + L::cx(i), nx), syy = wrap_idx(y + L::cy(i), ny),
                           szz = wrap_idx(z + L::cz(i), nz);
-                if (!solid_at(P, a.ivl, sxx, syy, szz)) continue;  // source x - c_j = x + c_i is fluid
+                const long long sc = sxx + (long long)nx * (syy + (long long)ny * szz);  // source x - c_j = x + c_i
+                const bool wlink = a.wall && a.wall[sc];
+                const bool plink = a.has_part && solid_at(P, a.ivl, sxx, syy, szz);
+                if (!wlink && !plink) continue;
                 const double cj[3] = {(double)L::cx(j), (double)L::cy(j), (double)L::cz(j)};
+                const double w6 = 6.0 * L::w(j);
+                const double lj = a.lam_in[j * N + cell];
+                // moving wall term 6 w_j rho c_j.u_w(x - c_j) (fluids.jl:167-174)
+                double cw = 0.0;
+                if (wlink && a.uw)
+                    for (int k = 0; k < D; ++k) cw += cj[k] * a.uw[(long long)k * N + sc];
+                if (!plink) {  // a wall link only: bounce-back copy and the wall term
+                    ls[i] += lj;
+                    mu_rho += lj * w6 * cw;
+                    continue;
+                }
                 const double ci[3] = {-cj[0], -cj[1], -cj[2]};
                 const double Y[3] = {a.coord[0][sxx], a.coord[1][syy], D == 3 ? a.coord[2][szz] : 0.0};
                 double up[3];
                 slip_velocity_t<D, double>(P.sR, P.sV, P.sW, P.sE, P.B1, P.B2, P.kind, Y[0], Y[1], Y[2], up);
-                const double cu = cj[0] * up[0] + cj[1] * up[1] + cj[2] * up[2];
-                const double w6 = 6.0 * L::w(j);
+                const double cu = cj[0] * up[0] + cj[1] * up[1] + cj[2] * up[2] + cw;  // Ladd and wall terms
                 const double s = 2.0 * fs[i] + w6 * rho * cu;  // f*_i + f^{n+1}_j
-                const double lj = a.lam_in[j * N + cell];
                 double lsi = lj, gmu = lj * w6 * cu, gup = lj * w6 * rho;  // lam_up = gup * c_j
                 if (P.coupleF || P.recordF) {
                     const double t = a.coeff * (a.lamF[0] * ci[0] + a.lamF[1] * ci[1] + a.lamF[2] * ci[2]);

@@ -3007,6 +3007,8 @@ int backward_tick(AdjointRun& R, long long n) {
     for (int k = 0; k < 3; ++k) a.coord[k] = h->d_coord[k];
     a.part = h->d_parts;
     a.ivl = h->d_ivl;
+    a.wall = h->d_wall;
+    a.uw = h->d_uw;
     a.has_part = 1;
     a.rho0 = h->rho0;
     a.inv_scale = 1.0 / h->scale;
@@ -3111,7 +3113,6 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
     if (h->particle_rules != LBM_RULES_GPU_MODULE)
         return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint follows the GPU module's particle update");
     if (!h->inter.empty()) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support particle interactions");
-    if (h->has_walls) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support walls");
     if (h->force_mode == LBM_FORCE_FIELD) return set_err(h, LBM_ERR_UNSUPPORTED, "the adjoint does not support force fields");
     if (spec->ticks < 1 || spec->window_begin < 1 || spec->window_end < spec->window_begin ||
         spec->window_end > spec->ticks)
