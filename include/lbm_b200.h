@@ -472,8 +472,10 @@ void lbm_batch_destroy(lbm_batch* b);
  * exchange) and of the particle update, recomputing forward segments from at
  * most `snapshots` stored states (binomial checkpointing).  The solid masks
  * are taken as the forward run computes them.  The handle is left in the
- * state it had on entry.  Requirements: one particle, no walls, no per-node
- * force field.  No counterpart in the reference (it has no differentiation). */
+ * state it had on entry.  Walls (static or moving) are differentiated
+ * through.  Requirements: one particle, the GPU module's particle rules, no
+ * interactions, no per-node force field.  No counterpart in the reference (it
+ * has no differentiation). */
 typedef struct lbm_adjoint_spec {
     int64_t ticks;
     int64_t window_begin, window_end;
