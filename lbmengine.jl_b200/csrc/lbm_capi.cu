@@ -367,6 +367,7 @@ StepArgs make_step_args(const lbm_handle* h, int src, double* partial) {
     }
     a.trt = h->trt;
     a.stochastic = h->rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
+    a.reverse = src;  // the tick after a forward pass (it wrote buffer 1) walks backwards
     fill_collide_consts(a);
     return a;
 }
@@ -2384,7 +2385,7 @@ void batch_enqueue(lbm_batch* b, int s) {
     // particle update is done; the particle update on the side stream
     if (b->tuning.tile_cta)
         b->ops.bulk_batch(b->d_targs + (size_t)s * b->reps.size(), b->d_dmap, b->nd, b->stream,
-                          b->reps[0]->rounding == LBM_ROUND_STOCHASTIC);
+                          b->reps[0]->rounding == LBM_ROUND_STOCHASTIC, s == 1);
     else
         batch_launch(b, s, batch_items(b, false, false, false, true, 0), 0, b->stream);
     if (b->part_pending) {

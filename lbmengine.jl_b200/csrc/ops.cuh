@@ -38,7 +38,7 @@ struct Ops {
     void (*tick)(const StepArgs* args, const ParticleArgs* pargs, const TickItems& items, TickCounters* q,
                  int* err, unsigned grid, cudaStream_t, bool sr);
     // a batch's bulk tiles, one CTA per entry of dmap
-    void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t, bool sr);
+    void (*bulk_batch)(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t, bool sr, bool reverse);
     // discrete adjoint of one tick, and of the initial condition (adjoint.cuh)
     void (*adjoint)(const AdjArgs&, cudaStream_t);
     void (*adjoint_init)(const AdjArgs&, cudaStream_t);
@@ -120,14 +120,15 @@ struct OpsImpl {
             k_tick<L, ST, TRT, false><<<grid, kTickBlock, 0, s>>>(args, pargs, items, q, err);
         }
     }
-    static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s, bool sr) {
+    static void bulk_batch(const StepArgs* args, const int2* dmap, long long tiles, cudaStream_t s, bool sr,
+                           bool reverse) {
         if constexpr (ST != ST_F64) {
             if constexpr (kTwo)
                 if (sr) {
-                    k_bulk_batch<L, ST, TRT, true><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+                    k_bulk_batch<L, ST, TRT, true><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap, reverse ? 1 : 0);
                     return;
                 }
-            k_bulk_batch<L, ST, TRT, false><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap);
+            k_bulk_batch<L, ST, TRT, false><<<(unsigned)tiles, kTickBlock, 0, s>>>(args, dmap, reverse ? 1 : 0);
         }
     }
     static void adjoint(const AdjArgs& a, cudaStream_t s) {

@@ -187,9 +187,10 @@ __global__ void __launch_bounds__(kTickBlock, 8) k_tick(const StepArgs* __restri
 // replicas' arguments come from `args[dmap[i].x]`.
 template <class L, int ST, bool TRT, bool SR>
 __global__ void __launch_bounds__(kTickBlock, bulk_threads_per_sm<L, ST, SR>() / kTickBlock)
-    k_bulk_batch(const StepArgs* __restrict__ args, const int2* __restrict__ dmap) {
+    k_bulk_batch(const StepArgs* __restrict__ args, const int2* __restrict__ dmap, int reverse) {
     __shared__ float s_ex[x_moving_dirs<L>()][kTickBlock];
-    const int2 m = dmap[blockIdx.x];
+    // every other tick the map is walked last to first (see k_bulk_v4)
+    const int2 m = dmap[reverse ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
     bulk_v4_tile<L, ST, TRT, kTickBlock, SR>(args[m.x], m.y, s_ex);
 }
 
