@@ -483,7 +483,8 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const StepArgs a) {
     using T = typename SS::T;
     using R = typename SS::R;
     constexpr int Q = L::Q;
-    const long long tile = blockIdx.x;
+    // every other tick the tiles run last to first, as in k_bulk_v4 (L2 reuse)
+    const long long tile = a.reverse ? a.g.ntiles - 1 - (long long)blockIdx.x : (long long)blockIdx.x;
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
     const int bx = (int)(tile % a.g.nt[0]);
     const int rr = (int)(tile / a.g.nt[0]);
