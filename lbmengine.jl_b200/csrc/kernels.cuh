@@ -726,10 +726,11 @@ __global__ void __launch_bounds__(B, bulk_threads_per_sm<L, ST, SR>() / B) k_bul
     __shared__ float s_ex[x_moving_dirs<L>()][B];
     grid_dep_trigger();  // the fix-up may start its stores-free part during the last wave
     const long long tiles = (long long)a.vnt1 * a.g.n[2];
-    // FP32: the last two fifths of the pass store with the default policy, so
-    // that L2 keeps those lines for the next pass (50.5 instead of 51.3 us per
-    // 128^3 tick); the issue-bound 2-byte passes measured slower with it
-    const bool keep = Store<ST>::bytes == 4 && (long long)blockIdx.x * 5 >= tiles * 3;
+    // FP32: the last three fifths of the pass store with the default policy,
+    // so that L2 keeps those lines for the next pass (128^3 tick: 51.3 us with
+    // none, 50.5 with two fifths, 49.4 with three, 50.2 with four, 51.6 with
+    // all); the issue-bound 2-byte passes measured slower with it
+    const bool keep = Store<ST>::bytes == 4 && (long long)blockIdx.x * 5 >= tiles * 2;
     bulk_v4_tile<L, ST, TRT, B, SR>(a, a.reverse ? tiles - 1 - (long long)blockIdx.x : (long long)blockIdx.x, s_ex,
                                     keep);
 }
