@@ -305,7 +305,7 @@ def run_ours(args):
                 "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "traffic_source": "replayed from an earlier ncu capture of consecutive live launches without cache "
-                                  "flushing (profiles/bulk_traffic.txt), not this run: each pass reads about 37 % "
+                                  "flushing (profiles/bulk_traffic.txt), not this run: each pass reads about 45 % "
                                   "(FP32) of its populations from L2, so DRAM traffic is below the algorithmic bytes",
                 "kernel": f"k_bulk_v4<D3Q19,{storage},TRT,64>", "bytes_per_launch": bulk_bytes,
                 "algorithmic_bytes_per_cell": 2 * q * bpp, "kernel_ms": kern,
