@@ -76,7 +76,9 @@ def bench_config(side, world):
             "ticks_valid": f"the squirmer crosses the periodic x boundary near tick {VALID_TICKS_128} (128^3), "
                            "after which the reference's unwrapped torque arm makes the coupling diverge",
             "parallelism": "replicas" if world > 1 else "single",
-            "l2": f"inputs larger than L2: D3Q19 populations 2 x {side ** 3 * 19 * 4 / 1e6:.0f} MB (FP32)"}
+            "l2": f"inputs larger than L2: D3Q19 populations 2 x {side ** 3 * 19 * 4 / 1e6:.0f} MB (FP32), no "
+                  "flush; each tick walks its tiles in the order opposite to the previous tick's and so reads "
+                  "part of its populations (about 45 % at 128^3 FP32) from what the previous tick left in L2"}
 
 
 def measured_peak():
