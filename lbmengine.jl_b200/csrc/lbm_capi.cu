@@ -184,6 +184,87 @@ int set_err(lbm_handle* h, int code, const std::string& msg) {
 // process-wide cap on the device bytes one handle or batch may hold (0: none)
 std::atomic<long long> g_mem_limit{0};
 
+// Device memory comes from one memory pool per device, owned by the library,
+// that keeps up to kPoolKeepBytes of freed memory for the next allocations:
+// cudaMalloc and cudaFree of a 128^3 D3Q19 FP32 model's buffers take about
+// 1.3 ms each, an allocation from kept memory about 20 us, so a process that
+// builds models one after another (parameter sweeps, replicas, the
+// end-to-end path of a short run) does not pay for them again.  Allocations
+// are made on the pool's own stream and waited for, so they are usable on any
+// stream; a free first waits for the device, as cudaFree does, so that no
+// queued work still uses the memory.  Pools and their streams live until the
+// process ends.
+constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
+constexpr int kMaxPoolDevices = 64;
+struct DevicePool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+std::mutex g_pool_mu;
+DevicePool g_pools[kMaxPoolDevices];
+
+cudaError_t device_pool(int dev, DevicePool** out) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+    DevicePool& d = g_pools[dev];
+    if (!d.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        unsigned long long keep = kPoolKeepBytes;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        cudaStream_t st = nullptr;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        d.pool = pool;
+        d.stream = st;
+    }
+    *out = &d;
+    return cudaSuccess;
+}
+
+// `bytes` (at least 1) from the current device's pool, ready for use on any stream
+cudaError_t pool_alloc(void** p, size_t bytes) {
+    int dev = 0;
+    DevicePool* d = nullptr;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = device_pool(dev, &d);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream);
+    if (e == cudaErrorMemoryAllocation) {  // hand the kept memory back and try once more
+        cudaGetLastError();
+        cudaStreamSynchronize(d->stream);
+        cudaMemPoolTrimTo(d->pool, 0);
+        e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    return e;
+}
+
+// back to the pool of the device that holds p, after that device's queued work
+void pool_free(void* p) {
+    cudaPointerAttributes at{};
+    int cur = 0;
+    DevicePool* d = nullptr;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || cudaGetDevice(&cur) != cudaSuccess ||
+        device_pool(at.device, &d) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    if (at.device != cur) cudaSetDevice(at.device);
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, d->stream);
+    if (at.device != cur) cudaSetDevice(cur);
+}
+
 template <class P>
 int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
     const long long cap = g_mem_limit.load();
@@ -193,7 +274,7 @@ int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
                                            " bytes would exceed the memory limit of " + std::to_string(cap) +
                                            " bytes (lbm_set_memory_limit)");
     }
-    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
+    cudaError_t e = pool_alloc((void**)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -206,7 +287,7 @@ int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
 
 template <class P>
 void dev_free(P*& p) {
-    if (p) cudaFree((void*)p);
+    if (p) pool_free((void*)p);
     p = nullptr;
 }
 
@@ -2262,7 +2343,7 @@ int bset_err(lbm_batch* b, int code, const std::string& msg) {
 
 template <class P>
 int bdev_alloc(lbm_batch* b, P** p, size_t bytes) {
-    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
+    cudaError_t e = pool_alloc((void**)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
