@@ -18,6 +18,8 @@
 #include <charconv>
 #include <chrono>
 #include <thread>
+#include <unordered_map>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -184,85 +186,108 @@ int set_err(lbm_handle* h, int code, const std::string& msg) {
 // process-wide cap on the device bytes one handle or batch may hold (0: none)
 std::atomic<long long> g_mem_limit{0};
 
-// Device memory comes from one memory pool per device, owned by the library,
-// that keeps up to kPoolKeepBytes of freed memory for the next allocations:
-// cudaMalloc and cudaFree of a 128^3 D3Q19 FP32 model's buffers take about
-// 1.3 ms each, an allocation from kept memory about 20 us, so a process that
-// builds models one after another (parameter sweeps, replicas, the
-// end-to-end path of a short run) does not pay for them again.  Allocations
-// are made on the pool's own stream and waited for, so they are usable on any
-// stream; a free first waits for the device, as cudaFree does, so that no
-// queued work still uses the memory.  Pools and their streams live until the
-// process ends.
-constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
-constexpr int kMaxPoolDevices = 64;
-struct DevicePool {
-    cudaMemPool_t pool = nullptr;
-    cudaStream_t stream = nullptr;
+// Device memory: cudaMalloc, with freed blocks kept (up to kKeepBytes over
+// all devices) for later allocations of the same size.  cudaMalloc and
+// cudaFree of a 128^3 D3Q19 FP32 model's buffers take about 1.3 ms each, a
+// kept block is handed out in microseconds, so a process that builds models
+// one after another (parameter sweeps, replicas, the end-to-end path of a
+// short run) does not pay for them again.  A stream-ordered memory pool gave
+// the same saving, but the bulk pass ran 1-1.5 % slower on its memory.  A
+// freed block is kept only after its device has finished its queued work,
+// as cudaFree waits for it.
+constexpr size_t kKeepBytes = size_t(4) << 30;
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<size_t, std::pair<int, void*>> kept;        // capacity -> (device, block)
+    std::unordered_map<void*, std::pair<int, size_t>> live;  // block -> (device, capacity)
+    size_t kept_bytes = 0;
 };
-std::mutex g_pool_mu;
-DevicePool g_pools[kMaxPoolDevices];
+BlockCache g_blocks;
 
-cudaError_t device_pool(int dev, DevicePool** out) {
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
-    DevicePool& d = g_pools[dev];
-    if (!d.pool) {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t pool = nullptr;
-        cudaError_t e = cudaMemPoolCreate(&pool, &props);
-        if (e != cudaSuccess) return e;
-        unsigned long long keep = kPoolKeepBytes;
-        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        cudaStream_t st = nullptr;
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-        if (e != cudaSuccess) {
-            cudaMemPoolDestroy(pool);
-            return e;
+// cudaFree the kept blocks of device `dev` (the current device)
+void release_kept(int dev) {
+    std::vector<void*> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_blocks.mu);
+        for (auto it = g_blocks.kept.begin(); it != g_blocks.kept.end();) {
+            if (it->second.first == dev) {
+                drop.push_back(it->second.second);
+                g_blocks.kept_bytes -= it->first;
+                it = g_blocks.kept.erase(it);
+            } else {
+                ++it;
+            }
         }
-        d.pool = pool;
-        d.stream = st;
     }
-    *out = &d;
-    return cudaSuccess;
+    for (void* q : drop) cudaFree(q);
 }
 
-// `bytes` (at least 1) from the current device's pool, ready for use on any stream
-cudaError_t pool_alloc(void** p, size_t bytes) {
+// `bytes` (at least 1) on the current device: a kept block of this device
+// holding them with at most an eighth to spare, else cudaMalloc
+cudaError_t block_alloc(void** p, size_t bytes) {
+    bytes = bytes ? bytes : 1;
     int dev = 0;
-    DevicePool* d = nullptr;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = device_pool(dev, &d);
     if (e != cudaSuccess) return e;
-    e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream);
-    if (e == cudaErrorMemoryAllocation) {  // hand the kept memory back and try once more
-        cudaGetLastError();
-        cudaStreamSynchronize(d->stream);
-        cudaMemPoolTrimTo(d->pool, 0);
-        e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream);
+    {
+        std::lock_guard<std::mutex> lk(g_blocks.mu);
+        for (auto it = g_blocks.kept.lower_bound(bytes);
+             it != g_blocks.kept.end() && it->first <= bytes + bytes / 8; ++it) {
+            if (it->second.first != dev) continue;
+            *p = it->second.second;
+            g_blocks.live[*p] = {dev, it->first};
+            g_blocks.kept_bytes -= it->first;
+            g_blocks.kept.erase(it);
+            return cudaSuccess;
+        }
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {  // hand this device's kept blocks back and try once more
+        cudaGetLastError();
+        release_kept(dev);
+        e = cudaMalloc(p, bytes);
+    }
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_blocks.mu);
+        g_blocks.live[*p] = {dev, bytes};
+    }
     return e;
 }
 
-// back to the pool of the device that holds p, after that device's queued work
-void pool_free(void* p) {
-    cudaPointerAttributes at{};
-    int cur = 0;
-    DevicePool* d = nullptr;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || cudaGetDevice(&cur) != cudaSuccess ||
-        device_pool(at.device, &d) != cudaSuccess) {
-        cudaGetLastError();
+// give back a block from block_alloc: kept when there is room, else cudaFree
+void block_free(void* p) {
+    int dev = -1;
+    size_t cap = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_blocks.mu);
+        auto it = g_blocks.live.find(p);
+        if (it != g_blocks.live.end()) {
+            dev = it->second.first;
+            cap = it->second.second;
+            g_blocks.live.erase(it);
+        }
+    }
+    if (dev < 0) {
         cudaFree(p);
         return;
     }
-    if (at.device != cur) cudaSetDevice(at.device);
-    cudaDeviceSynchronize();
-    cudaFreeAsync(p, d->stream);
-    if (at.device != cur) cudaSetDevice(cur);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (dev != cur) cudaSetDevice(dev);
+    bool kept = false;
+    if (cudaDeviceSynchronize() == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_blocks.mu);
+        if (g_blocks.kept_bytes + cap <= kKeepBytes) {
+            g_blocks.kept.emplace(cap, std::make_pair(dev, p));
+            g_blocks.kept_bytes += cap;
+            kept = true;
+        }
+    }
+    if (!kept) {
+        cudaGetLastError();
+        cudaFree(p);
+    }
+    if (dev != cur) cudaSetDevice(cur);
 }
 
 template <class P>
@@ -274,7 +299,7 @@ int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
                                            " bytes would exceed the memory limit of " + std::to_string(cap) +
                                            " bytes (lbm_set_memory_limit)");
     }
-    cudaError_t e = pool_alloc((void**)p, bytes);
+    cudaError_t e = block_alloc((void**)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -287,7 +312,7 @@ int dev_alloc(lbm_handle* h, P** p, size_t bytes) {
 
 template <class P>
 void dev_free(P*& p) {
-    if (p) pool_free((void*)p);
+    if (p) block_free((void*)p);
     p = nullptr;
 }
 
@@ -2343,7 +2368,7 @@ int bset_err(lbm_batch* b, int code, const std::string& msg) {
 
 template <class P>
 int bdev_alloc(lbm_batch* b, P** p, size_t bytes) {
-    cudaError_t e = pool_alloc((void**)p, bytes);
+    cudaError_t e = block_alloc((void**)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
