@@ -369,8 +369,10 @@ def run_ours(args):
            "path": "modelInit with pinned column-major host rho/u (lbm_create) + addSquirmer + LBMpropagate in "
                    f"blocks of up to {ring} ticks, each block's per-tick particle states read from the device "
                    "trajectory ring (lbm_read_trajectories), then massDensity/fluidVelocity into pinned host "
-                   "arrays (lbm_get_fields); host wall clock, including the model's graph builds, after one "
-                   "untimed 2-tick pass of the same calls"}
+                   "arrays (lbm_get_fields); host wall clock, including any graph builds (a model's first call "
+                   "of up to 32 ticks launches its ticks directly, later calls build the graphs they need), after "
+                   "one untimed 2-tick pass of the same calls (whose freed device blocks the library keeps for "
+                   "reuse, as for any model built after another in a process)"}
     del keep
 
     cpu = None
