@@ -45,7 +45,11 @@ def julia_float_range(start, stop, step):
     fs, ft, fp = _exact_fraction(start), _exact_fraction(stop), _exact_fraction(step)
     if fs is not None and ft is not None and fp is not None:
         length = max(0, math.floor((ft - fs) / fp) + 1)
-        return np.array([float(fs + i * fp) for i in range(length)], dtype=np.float64)
+        # start + i*step = (a d + i c b) / (b d) for start = a/b, step = c/d;
+        # int / int is correctly rounded, as float(Fraction) is
+        a, b, c, d = fs.numerator, fs.denominator, fp.numerator, fp.denominator
+        num0, dnum, den = a * d, c * b, b * d
+        return np.array([(num0 + i * dnum) / den for i in range(length)], dtype=np.float64)
     lf = (stop - start) / step
     if lf < 0:
         length = 0

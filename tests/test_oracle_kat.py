@@ -150,6 +150,28 @@ def test_squirmer_keyword_resolution_quirks():
         config.resolve_squirmer(2, B1=1.0, B2=1.0, beta=1.0)
 
 
+def test_julia_range_elements_are_the_rounded_rationals():
+    """julia_float_range with exact rational start/step/stop: element i is the
+    correctly rounded start + i*step (base/twiceprecision.jl), computed as one
+    integer division; checked against Fraction arithmetic bit for bit."""
+    rng = np.random.default_rng(7)
+    checked = 0
+    for _ in range(3000):
+        dx = float(rng.choice([1.0, 0.1, 0.01, 0.5, 0.3, 1 / 3, 0.7, 0.05, 2.5, 1e-3, 0.2]))
+        start = float(rng.choice([-64.0, -63.5, 0.0, -0.5, round(float(rng.uniform(-100, 100)), 2)]))
+        stop = start + int(rng.integers(1, 300)) * dx + float(rng.choice([0.0, 1e-9, -1e-9]))
+        fr = [config._exact_fraction(v) for v in (start, stop, dx)]
+        if any(f is None for f in fr):
+            continue
+        fs, ft, fp = fr
+        n = max(0, math.floor((ft - fs) / fp) + 1)
+        want = np.array([float(fs + i * fp) for i in range(n)])
+        got = config.julia_float_range(start, stop, dx)
+        assert got.shape == want.shape and np.array_equal(got.view(np.int64), want.view(np.int64))
+        checked += 1
+    assert checked > 1000
+
+
 def _numpy_mask(coords, R, r):
     grids = np.meshgrid(*coords, indexing="ij")
     s = (grids[0] - R[0]) * (grids[0] - R[0]) + (grids[1] - R[1]) * (grids[1] - R[1])
