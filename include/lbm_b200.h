@@ -538,6 +538,11 @@ int lbm_adjoint(lbm_handle* h, const lbm_adjoint_spec* spec, lbm_adjoint_result*
 #define LBM_NOALLOC_SLOTS 16384
 int lbm_step_noalloc(lbm_handle* h, int64_t nsteps);
 
+/* lbm_destroy waits for the handle's queued work and gives its device
+ * buffers back.  The library keeps freed device blocks (up to 4 GiB in the
+ * process) for later allocations of the same size, so a model built after
+ * another does not pay cudaMalloc again; the kept blocks go back to the
+ * driver when a cudaMalloc fails. */
 const char* lbm_last_error(lbm_handle* h);
 const char* lbm_last_global_error(void);
 void lbm_destroy(lbm_handle* h);
